@@ -1,0 +1,124 @@
+// nf_pair.cuh -- per-pair softened gravity on the B200 FP32 pipe.
+//
+// Softening formulas follow singlestep/Direct/DirectGPUKernels.cuh:20-174
+// (Plummer :144-174, single spline :68-108, cubic spline :20-66, cubic
+// Plummer :110-143).  Differences from the reference GPU kernel, all in the
+// direction of accuracy:
+//   * rsqrt is the hardware estimate (rsqrt.approx.ftz.f32) followed by one
+//     Newton-Raphson step; for the far field the step is applied to the cube:
+//       y = rsqrt(r2); e = r2*y^2 - 1; r2^-3/2 ~= y^3 * (1 - 1.5 e)
+//     (first-order Newton correction of y, cubed: 5 FP32 instructions).
+//   * the single spline's far branch is accumulated without the 1/eps^2
+//     scaling (g = r^-3, the result is multiplied by eps^3 once per sink);
+//     pairs closer than the softening length take the reference formula,
+//     min(f^3, (-15 f + 6) dr2 + 10) (the fminf form of DirectCPUKernels.cc:71),
+//     times eps^-3.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace nf {
+
+enum { SOFT_PLUMMER = 0, SOFT_SINGLE_SPLINE = 1, SOFT_CUBIC_SPLINE = 2, SOFT_CUBIC_PLUMMER = 3 };
+
+// Hardware reciprocal square root estimate (one MUFU.RSQ).
+__device__ __forceinline__ float rsqrt_est(float x) {
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// r2^-3/2 from the estimate plus one Newton step on the cube.
+__device__ __forceinline__ float inv_r3(float r2) {
+    float y = rsqrt_est(r2);
+    float y2 = y * y;
+    float y3 = y2 * y;
+    float e = fmaf(r2, y2, -1.0f);
+    float g = y3 * e;
+    return fmaf(g, -1.5f, y3);
+}
+
+// rsqrt with one Newton step: y (1.5 - 0.5 x y^2).
+__device__ __forceinline__ float rsqrt_nr(float x) {
+    float y = rsqrt_est(x);
+    float h = x * y;
+    float e = fmaf(-h, y, 1.0f);
+    return fmaf(0.5f * y, e, y);
+}
+
+// TwoSum (Knuth): s + err == a + b exactly.
+__device__ __forceinline__ void two_sum(float a, float b, float &s, float &err) {
+    s = a + b;
+    float bb = s - a;
+    err = (a - (s - bb)) + (b - bb);
+}
+
+// Kernel constants shared by every pair of a launch.
+struct PairConst {
+    float eps;        // the reference kernel parameter (eps^2, 1/eps^2, 1/eps, eps^3)
+    float near_thr;   // single spline: r^2 below which the exact formula is used
+    float inv_eps3;   // single spline: eps^-3
+    float b2;         // FOF density radius^2 (0 = off)
+};
+
+// Far-field / default evaluation: returns g with a -= g * d.
+// Plummer: (r^2 + eps^2)^-3/2.  Single spline far branch: r^-3 (r^2 floored
+// at 1e-25 so that a self pair stays finite; it is always re-evaluated by
+// the exact path because its r^2 is below near_thr).
+template <int SOFT>
+__device__ __forceinline__ float pair_g_fast(float dx, float dy, float dz, const PairConst &pc,
+                                             float &r2_out) {
+    if (SOFT == SOFT_PLUMMER) {
+        float r2 = fmaf(dz, dz, fmaf(dy, dy, fmaf(dx, dx, pc.eps)));
+        r2_out = r2;
+        return inv_r3(r2);
+    } else if (SOFT == SOFT_SINGLE_SPLINE) {
+        float r2 = fmaf(dz, dz, fmaf(dy, dy, fmaf(dx, dx, 1e-25f)));
+        r2_out = r2;
+        return inv_r3(r2);
+    } else if (SOFT == SOFT_CUBIC_SPLINE) {
+        // Hernquist & Katz cubic spline, DirectGPUKernels.cuh:31-65.
+        float r2 = fmaf(dz, dz, fmaf(dy, dy, fmaf(dx, dx, 1e-30f)));
+        r2_out = r2;
+        float rinv = rsqrt_nr(r2);
+        float u = pc.eps / rinv;
+        float r3 = rinv * rinv * rinv;
+        float spf;
+        if (u >= 2.0f) {
+            spf = r3;
+        } else if (u >= 1.0f) {
+            float u3 = u * u * u;
+            spf = r3 * (-1.0f / 15.0f + (8.0f / 3.0f) * u3 - 3.0f * u3 * u +
+                        (6.0f / 5.0f) * u3 * u * u - (1.0f / 6.0f) * u3 * u3);
+        } else {
+            float ei3 = pc.eps * pc.eps * pc.eps;
+            spf = ei3 * ((4.0f / 3.0f) - (6.0f / 5.0f) * u * u + 0.5f * u * u * u);
+        }
+        return spf;
+    } else {
+        // cubic Plummer, DirectGPUKernels.cuh:124-143 (TAU2 = 1e-16).
+        float r = fmaf(dz, dz, fmaf(dy, dy, fmaf(dx, dx, 1e-16f)));
+        r2_out = r;
+        float r3 = r * r * rsqrt_nr(r);
+        return 1.0f / (r3 + pc.eps);
+    }
+}
+
+// Single spline, exact reference formula in far units (g * eps^3 = f_ref).
+__device__ __forceinline__ float spline_g_exact(float dx, float dy, float dz,
+                                                const PairConst &pc) {
+    float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+    float dr2 = fmaf(r2, pc.eps, 1e-32f);
+    float f = rsqrt_nr(dr2);
+    float f3 = f * f * f;  // +inf for a self pair; the min picks the polynomial
+    float pn = fmaf(fmaf(-15.0f, f, 6.0f), dr2, 10.0f);
+    return fminf(f3, pn) * pc.inv_eps3;
+}
+
+// Unsoftened r^2 for the FOF density sum (w += b2 - r^2 if r^2 < b2).
+__device__ __forceinline__ float dens_term(float dx, float dy, float dz, float b2) {
+    float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+    return r2 < b2 ? b2 - r2 : 0.0f;
+}
+
+}  // namespace nf

@@ -1,0 +1,443 @@
+"""Near-field direct-force benchmark (one JSON line on stdout, rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload clustered256|uniform64|clustered512]
+
+A step is one full near-field sweep of a synthetic box (every sink of every
+x-slab against its 5x5x5 cell neighbourhood), the box's positions already
+resident in HBM.  The default workload is the clustered box: 256^3 particles,
+cpd 65, 40% uniform + 60% in 2000 seeded NFW clumps, single-spline softening
+at 1/40 of the mean spacing, float32, compensated accumulation.
+
+metric: pair interactions/s (unpadded pairs, PencilOnPencil.cc:412 counting),
+plus p50/p99 slab latency.  Multi-GPU (torchrun): every rank sweeps its own
+independent box of the same configuration (weak scaling, no data-path
+collective); the timed region is bracketed by a barrier and the time is the
+max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+FLOPS_PER_PAIR = {0: 23, 1: 24, 2: 24, 3: 24}  # counted flops (FFMA=2, rsqrt=1, Newton incl.)
+
+
+def _pkg():
+    import importlib.util
+    if "abacus_public_b200" not in sys.modules:
+        spec = importlib.util.spec_from_file_location(
+            "abacus_public_b200", ROOT / "abacus-public_b200" / "__init__.py",
+            submodule_search_locations=[str(ROOT / "abacus-public_b200")])
+        mod = importlib.util.module_from_spec(spec)
+        sys.modules["abacus_public_b200"] = mod
+        spec.loader.exec_module(mod)
+    return sys.modules["abacus_public_b200"]
+
+
+WORKLOADS = {
+    "clustered256": dict(n_side=256, cpd=65, softening=1, kind="clustered", seed=2,
+                         desc="256^3 particles, cpd 65, 40% uniform + 60% in 2000 NFW clumps "
+                              "(c=10, r_t=0.6 cell), single spline eps_pl=spacing/40"),
+    "uniform64": dict(n_side=64, cpd=17, softening=0, kind="uniform", seed=1,
+                      desc="64^3 uniform particles, cpd 17, Plummer eps=spacing/40"),
+    "clustered512": dict(n_side=512, cpd=125, softening=1, kind="clustered", seed=3,
+                         desc="512^3 particles, cpd 125, clustered mixture as clustered256"),
+}
+
+
+def make_box(w, seed_offset=0):
+    _pkg()
+    from abacus_public_b200 import synth
+    n = w["n_side"] ** 3
+    if w["kind"] == "uniform":
+        return synth.uniform_box(n, w["cpd"], w["seed"] + seed_offset)
+    return synth.clustered_box(n, w["cpd"], w["seed"] + seed_offset)
+
+
+def kernel_eps(w):
+    from abacus_public_b200 import synth
+    return synth.kernel_eps(w["softening"], synth.plummer_eps(w["n_side"]))
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.path)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing
+# ---------------------------------------------------------------------------
+def dist_init(n_gpus):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return rank, world, local
+
+
+def barrier_max(value: float, world: int) -> float:
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def all_sum(value: float, world: int) -> float:
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the reference's own kernel compiled from its sources
+# (oracle/_ref, -Ofast), driven by the ExecuteSlabCPU cell loop
+# ---------------------------------------------------------------------------
+def cpu_reference_rate(box, w, target_s=10.0, seed=0):
+    """Pairs/s of the reference CPU direct on a seeded sample of sink cells,
+    all host threads.  Returns (rate, threads, sample description, kind)."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+    soft = w["softening"]
+    eps = kernel_eps(w)
+    threads = oracle.host_threads()
+    if oracle.have_ref(soft, "fast"):
+        kind = "reference"
+
+        def run(cells):
+            oracle.ref_cells(box, soft, eps, cells, flavour="fast", threads=threads)
+    else:
+        kind = "port"
+
+        def run(cells):
+            oracle.ref32_cells(box, soft, eps, cells)
+    counts = box.counts
+    ncell = counts.size
+    cpd = box.cpd
+    rng = np.random.default_rng(seed)
+    order = rng.permutation(np.nonzero(counts)[0])
+
+    def pairs_of(cells):
+        tot = 0
+        c3 = counts.reshape(cpd, cpd, cpd)
+        for c in cells:
+            cz, cy, cx = c % cpd, (c // cpd) % cpd, c // (cpd * cpd)
+            xs = [(cx + d) % cpd for d in range(-2, 3)]
+            ys = [(cy + d) % cpd for d in range(-2, 3)]
+            zs = [(cz + d) % cpd for d in range(-2, 3)]
+            tot += int(counts[c]) * int(c3[np.ix_(xs, ys, zs)].sum())
+        return tot
+
+    # calibrate on a small sample, then size the sample to ~target_s
+    n = max(threads * 4, 64)
+    cells = order[:n]
+    t0 = time.perf_counter()
+    run(cells)
+    dt = time.perf_counter() - t0
+    p = pairs_of(cells)
+    rate0 = p / max(dt, 1e-9)
+    want = rate0 * target_s
+    k = n
+    acc = p
+    while acc < want and k < ncell:
+        step = order[k:k + 4096]
+        acc += pairs_of(step)
+        k += step.size
+    cells = order[:k]
+    t0 = time.perf_counter()
+    run(cells)
+    dt = time.perf_counter() - t0
+    pairs = pairs_of(cells)
+    desc = (f"{k} seeded random non-empty sink cells of the same box "
+            f"({pairs:.3e} pairs, {dt:.1f} s), {threads} threads")
+    return pairs / dt, threads, desc, kind, pairs, dt
+
+
+def reference_arm(args, w):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    box = make_box(w)
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+    soft = w["softening"]
+    eps = kernel_eps(w)
+    threads = oracle.host_threads()
+    flavour_ok = oracle.have_ref(soft, "fast")
+    # per step: a fixed seeded sample of sink cells sized to ~6 s on this host
+    rate, threads, desc, kind, pairs, dt = cpu_reference_rate(box, w, target_s=6.0, seed=123)
+    counts = box.counts
+    rng = np.random.default_rng(123)
+    order = rng.permutation(np.nonzero(counts)[0])
+    ncells = int(desc.split()[0])
+    cells = order[:ncells]
+    times = []
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        if flavour_ok:
+            oracle.ref_cells(box, soft, eps, cells, flavour="fast", threads=threads)
+        else:
+            oracle.ref32_cells(box, soft, eps, cells)
+        if i >= args.warmup:
+            times.append(time.perf_counter() - t0)
+    ms = 1e3 * sum(times) / len(times)
+    value = pairs / (ms / 1e3)
+    line = {
+        "impl": "reference", "metric": "pair_interactions_per_s", "value": value,
+        "unit": "pairs/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.workload, "desc": w["desc"],
+                   "step": "a seeded sample of sink cells of the box (the reference CPU "
+                           "direct is too slow for whole sweeps)"},
+        "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": threads, "kind": kind,
+                         "sample": desc},
+        "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def percentile(xs, q):
+    return float(np.percentile(np.asarray(xs), q)) if xs else None
+
+
+def our_arm(args, w):
+    import torch
+    rank, world, local = dist_init(args.gpus)
+    _pkg()
+    from abacus_public_b200 import capi
+    box = make_box(w, seed_offset=rank)
+    eps = kernel_eps(w)
+    soft = w["softening"]
+    ctx = capi.Context(softening=soft, eps=eps, device=local)
+    torch.cuda.set_device(local)
+    stream = torch.cuda.Stream(device=local)
+    torch.cuda.set_stream(stream)
+    ctx.set_stream(stream.cuda_stream)  # the library launches on the stream the events time
+    peak_burst, peak_sust = ctx.fp32_peak(1.0)
+    db = ctx.box(box)
+    pairs = db.pair_count()
+    n = box.n
+    out_dev = torch.empty((n, 4), dtype=torch.float32, device=f"cuda:{local}")
+    # warm-up (graph capture happens on the first call)
+    for _ in range(args.warmup):
+        db.forces_device(0, box.cpd, out_dev.data_ptr())
+    torch.cuda.synchronize()
+    kernel_ms, step_ms_dev = [], []
+    with ClockSampler(local) as clk:
+        barrier(world)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            db.forces_device(0, box.cpd, out_dev.data_ptr())
+            t = ctx.last_timing()
+            kernel_ms.append(t.kernel_ms)
+            step_ms_dev.append(t.total_ms)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier(world)
+        elapsed = e0.elapsed_time(e1)
+    clocks = clk.summary()
+    elapsed = barrier_max(elapsed, world)
+    ms_per_step = elapsed / args.steps
+    total_pairs = all_sum(float(pairs), world)
+    value = total_pairs / (ms_per_step / 1e3)
+    launches = args.steps * t.launches
+
+    # end to end through the C ABI with pinned host buffers: H2D positions,
+    # sweep, D2H accelerations, every step
+    hx = torch.from_numpy(box.x).pin_memory()
+    hy = torch.from_numpy(box.y).pin_memory()
+    hz = torch.from_numpy(box.z).pin_memory()
+    hout = torch.empty((n, 4), dtype=torch.float32).pin_memory()
+    xa, ya, za, oa = hx.numpy(), hy.numpy(), hz.numpy(), hout.numpy()
+    db.update(xa, ya, za)
+    db.forces(0, box.cpd, out=oa)
+    barrier(world)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        db.update(xa, ya, za)
+        db.forces(0, box.cpd, out=oa)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = barrier_max(e0.elapsed_time(e1) / args.steps, world)
+    e2e_value = total_pairs / (e2e_ms / 1e3)
+
+    # slab latency: one request per x-slab, result in the caller's device buffer
+    lat = []
+    for s in range(box.cpd):
+        p0, p1 = db.slab_particles(s, s + 1)
+        db.forces_device(s, s + 1, out_dev.data_ptr())  # warm the slab's graph
+    for rep in range(2):
+        for s in range(box.cpd):
+            t0 = time.perf_counter()
+            db.forces_device(s, s + 1, out_dev.data_ptr())
+            lat.append(1e3 * (time.perf_counter() - t0))
+
+    flops = FLOPS_PER_PAIR[soft]
+    k_ms = float(np.mean(kernel_ms))
+    achieved = pairs * flops / (k_ms / 1e3) / 1e12
+    traffic = None
+    prof = ROOT / "profiles" / f"pencil_kernel_{args.workload}.json"
+    if prof.exists():
+        try:
+            traffic = json.loads(prof.read_text()).get("dram_bytes_per_launch")
+        except (ValueError, OSError):
+            traffic = None
+    result = {
+        "metric": "pair_interactions_per_s", "value": value, "unit": "pairs/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": args.workload, "desc": w["desc"], "particles_per_gpu": n,
+                   "cpd": box.cpd, "pairs_per_step_per_gpu": pairs,
+                   "padded_pairs_per_step_per_gpu": int(t.padded_pairs),
+                   "accumulation": "compensated",
+                   "l2": "inputs larger than L2 (positions 16 B x N + 120 B x N partials)",
+                   "parallelism": f"independent boxes x{world}"},
+        "slab_latency_ms": {"p50": percentile(lat, 50), "p99": percentile(lat, 99),
+                            "n": len(lat), "what": "one x-slab request, call to result in "
+                                                  "the caller's device buffer"},
+        "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak_sust, "unit": "TFLOP/s",
+                     "frac": achieved / peak_sust, "traffic": traffic,
+                     "kernel": "pencil_kernel", "kernel_ms": k_ms,
+                     "flops_per_pair": flops,
+                     "peak_source": "FFMA microbenchmark on this GPU in this run, sustained "
+                                    "(MEASURED_PEAKS.json has no FP32 figure)",
+                     "peak_burst": peak_burst},
+        "e2e": {"value": e2e_value, "unit": "pairs/s", "ms_per_step": e2e_ms,
+                "h2d_bytes_per_step": int(12 * n), "d2h_bytes_per_step": int(16 * n)},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        rate, threads, desc, kind, _, _ = cpu_reference_rate(box, w, target_s=args.cpu_seconds)
+        result["cpu_baseline"] = {"value": rate, "unit": "pairs/s", "cores": threads,
+                                  "kind": kind, "sample": desc}
+        # precision of this run's result against the FP64 oracle (checker)
+        sys.path.insert(0, str(ROOT / "oracle"))
+        import oracle
+        a = out_dev.cpu().numpy()
+        sinks = np.sort(np.random.default_rng(5).choice(n, 2000, replace=False))
+        rms, mx, _ = oracle.frac_errors(a[sinks, :3], oracle.fp64_sinks(box, soft, eps, sinks))
+        result["accuracy_vs_fp64"] = {"rms_frac": rms, "max_frac": mx, "sinks": 2000}
+    db.close()
+    ctx.close()
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="clustered256")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    w = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        return reference_arm(args, w)
+    return our_arm(args, w)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

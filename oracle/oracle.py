@@ -1,0 +1,173 @@
+"""ctypes front end of the oracle (TEST INFRASTRUCTURE ONLY).
+
+Loads oracle/liboracle.so (the C restatement in nf_oracle.c) and, when it was
+built, oracle/_ref/libnfref_<softening>.so (the reference's own
+singlestep/Direct/direct.cpp + DirectCPUKernels.cc compiled unmodified from
+its sources, driven by the ExecuteSlabCPU cell loop in ref_shim.cpp).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
+this module; the product library never does.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import pathlib
+
+import numpy as np
+
+HERE = pathlib.Path(__file__).resolve().parent
+LIB = HERE / "liboracle.so"
+REF_DIR = HERE / "_ref"
+SOFTENING_NAMES = {0: "plummer", 1: "single_spline", 2: "cubic_spline", 3: "cubic_plummer"}
+
+_i64p = np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")
+_f32p = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+
+_lib = None
+_ref = {}
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not LIB.exists():
+            raise FileNotFoundError(f"{LIB} is not built (run __graft_entry__.build())")
+        L = ctypes.CDLL(str(LIB))
+        L.nfo_ref32_slab.argtypes = [ctypes.c_int, ctypes.c_int, _i64p, _f32p, _f32p, _f32p,
+                                     ctypes.c_int, ctypes.c_float, ctypes.c_int, _f32p]
+        L.nfo_ref32_cells.argtypes = [ctypes.c_int, ctypes.c_int, _i64p, _f32p, _f32p, _f32p,
+                                      ctypes.c_int, ctypes.c_float, _i64p, ctypes.c_int64, _f32p]
+        L.nfo_fp64_sinks.argtypes = [ctypes.c_int, ctypes.c_int, _i64p, _f32p, _f32p, _f32p,
+                                     ctypes.c_int, ctypes.c_double, _i64p, ctypes.c_int64, _f64p]
+        L.nfo_frame32_sinks.argtypes = [ctypes.c_int, ctypes.c_int, _i64p, _f32p, _f32p, _f32p,
+                                        ctypes.c_int, ctypes.c_float, ctypes.c_int, _i64p,
+                                        ctypes.c_int64, _f32p]
+        L.nfo_fp64_density.argtypes = [ctypes.c_int, ctypes.c_int, _i64p, _f32p, _f32p, _f32p,
+                                       ctypes.c_double, _i64p, ctypes.c_int64, _f64p]
+        L.nfo_fp64_density.restype = ctypes.c_int
+        L.nfo_pair_count.argtypes = [ctypes.c_int, ctypes.c_int, _i64p]
+        L.nfo_pair_count.restype = ctypes.c_uint64
+        for f in (L.nfo_ref32_slab, L.nfo_ref32_cells, L.nfo_fp64_sinks, L.nfo_frame32_sinks):
+            f.restype = ctypes.c_int
+        _lib = L
+    return _lib
+
+
+def _check(rc):
+    if rc != 0:
+        raise ValueError(f"oracle call failed with {rc}")
+
+
+def ref32_slab(box, softening, eps, slab, R=2, acc=None):
+    """Reference CPU direct (restated) for every sink of one x-slab.
+    Returns float32[N,3] with only the slab's rows written."""
+    if acc is None:
+        acc = np.zeros((box.n, 3), dtype=np.float32)
+    _check(lib().nfo_ref32_slab(box.cpd, R, box.cell_start, box.x, box.y, box.z,
+                                softening, eps, slab, acc.reshape(-1)))
+    return acc
+
+
+def ref32_cells(box, softening, eps, cells, R=2, acc=None):
+    if acc is None:
+        acc = np.zeros((box.n, 3), dtype=np.float32)
+    cells = np.ascontiguousarray(cells, dtype=np.int64)
+    _check(lib().nfo_ref32_cells(box.cpd, R, box.cell_start, box.x, box.y, box.z,
+                                 softening, eps, cells, cells.size, acc.reshape(-1)))
+    return acc
+
+
+def fp64_sinks(box, softening, eps, sinks, R=2):
+    sinks = np.ascontiguousarray(sinks, dtype=np.int64)
+    out = np.zeros((sinks.size, 3), dtype=np.float64)
+    _check(lib().nfo_fp64_sinks(box.cpd, R, box.cell_start, box.x, box.y, box.z, softening,
+                                float(np.float32(eps)), sinks, sinks.size, out.reshape(-1)))
+    return out
+
+
+def fp64_density(box, b2, sinks, R=2):
+    sinks = np.ascontiguousarray(sinks, dtype=np.int64)
+    out = np.zeros(sinks.size, dtype=np.float64)
+    _check(lib().nfo_fp64_density(box.cpd, R, box.cell_start, box.x, box.y, box.z,
+                                  float(np.float32(b2)), sinks, sinks.size, out))
+    return out
+
+
+def frame32_sinks(box, softening, eps, sinks, compensated=True, R=2):
+    sinks = np.ascontiguousarray(sinks, dtype=np.int64)
+    out = np.zeros((sinks.size, 3), dtype=np.float32)
+    _check(lib().nfo_frame32_sinks(box.cpd, R, box.cell_start, box.x, box.y, box.z, softening,
+                                   eps, int(compensated), sinks, sinks.size, out.reshape(-1)))
+    return out
+
+
+def pair_count(box, R=2) -> int:
+    return int(lib().nfo_pair_count(box.cpd, R, box.cell_start))
+
+
+def frac_errors(a, a64):
+    """Per-sink fractional force error |a - a64| / |a64| (as in
+    Tests/Ewald/run_ewald.py:268) -> (rms, max, per-sink array)."""
+    a = np.asarray(a, dtype=np.float64)
+    num = np.linalg.norm(a - a64, axis=1)
+    den = np.linalg.norm(a64, axis=1)
+    ok = den > 0
+    e = np.zeros_like(num)
+    e[ok] = num[ok] / den[ok]
+    return float(np.sqrt(np.mean(e[ok] ** 2))) if ok.any() else 0.0, float(e.max()), e
+
+
+# ---------------------------------------------------------------------------
+# the reference's own kernel, compiled from its sources (oracle/_ref)
+# ---------------------------------------------------------------------------
+
+def ref_lib_path(softening: int, flavour: str = "strict") -> pathlib.Path:
+    return REF_DIR / f"libnfref_{SOFTENING_NAMES[softening]}_{flavour}.so"
+
+
+def have_ref(softening: int, flavour: str = "strict") -> bool:
+    return ref_lib_path(softening, flavour).exists()
+
+
+def ref_lib(softening: int, flavour: str = "strict"):
+    key = (softening, flavour)
+    if key not in _ref:
+        L = ctypes.CDLL(str(ref_lib_path(softening, flavour)))
+        L.nfref_execute_slab.argtypes = [ctypes.c_int, ctypes.c_int, _i64p, _f32p, _f32p, _f32p,
+                                         ctypes.c_float, ctypes.c_int, _f32p, ctypes.c_int]
+        L.nfref_execute_slab.restype = ctypes.c_int
+        L.nfref_execute_cells.argtypes = [ctypes.c_int, ctypes.c_int, _i64p, _f32p, _f32p, _f32p,
+                                          ctypes.c_float, _i64p, ctypes.c_int64, _f32p,
+                                          ctypes.c_int]
+        L.nfref_execute_cells.restype = ctypes.c_int
+        L.nfref_max_threads.restype = ctypes.c_int
+        _ref[key] = L
+    return _ref[key]
+
+
+def ref_slab(box, softening, eps, slab, R=2, flavour="strict", threads=0, acc=None):
+    """The reference's Direct::Execute over one slab (ExecuteSlabCPU loop)."""
+    if acc is None:
+        acc = np.zeros((box.n, 3), dtype=np.float32)
+    _check(ref_lib(softening, flavour).nfref_execute_slab(
+        box.cpd, R, box.cell_start, box.x, box.y, box.z, eps, slab, acc.reshape(-1), threads))
+    return acc
+
+
+def ref_cells(box, softening, eps, cells, R=2, flavour="strict", threads=0, acc=None):
+    if acc is None:
+        acc = np.zeros((box.n, 3), dtype=np.float32)
+    cells = np.ascontiguousarray(cells, dtype=np.int64)
+    _check(ref_lib(softening, flavour).nfref_execute_cells(
+        box.cpd, R, box.cell_start, box.x, box.y, box.z, eps, cells, cells.size,
+        acc.reshape(-1), threads))
+    return acc
+
+
+def host_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:  # pragma: no cover
+        return os.cpu_count() or 1

@@ -1,0 +1,210 @@
+"""Parity of the batched B200 path (nf_box_forces, through the C ABI) with
+the oracle.
+
+Tolerances (stated once, used below):
+  * against the reference's own CPU direct (golden vectors / oracle
+    restatement): for every sink and component |a_k - a_ref,k| <= 1e-4 |a_ref|,
+    and RMS over sinks of |a - a_ref| / |a_ref| <= 5e-6.  The reference itself
+    carries ~1e-6 RMS FP32 error (shifted frames, long FP32 running sums), so
+    bit equality with it is neither expected nor desirable.
+  * against the FP64 oracle: RMS fractional force error <= 2e-6 (the
+    acceptance bar), and max <= 1e-4.
+  * the FOF density channel w: relative 1e-5 against FP64.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN_TOL_COMP = 1e-4
+GOLDEN_TOL_RMS = 5e-6
+FP64_RMS = 2e-6
+FP64_MAX = 1e-4
+
+
+def _golden(path):
+    f = np.load(path)
+    from abacus_public_b200 import synth
+    box = synth.Box(cpd=int(f["cpd"]), x=f["x"], y=f["y"], z=f["z"], cell_start=f["cell_start"])
+    return box, int(f["softening"]), float(f["eps"]), list(f["slabs"]), f["rows"], f["acc"]
+
+
+def _check_vs_ref(a, ref):
+    norm = np.linalg.norm(ref.astype(np.float64), axis=1)
+    ok = norm > 0
+    diff = np.abs(a[:, :3].astype(np.float64) - ref)
+    assert np.all(diff[ok] <= GOLDEN_TOL_COMP * norm[ok, None]), \
+        float((diff[ok] / norm[ok, None]).max())
+    rel = np.linalg.norm(diff, axis=1)[ok] / norm[ok]
+    assert np.sqrt(np.mean(rel ** 2)) <= GOLDEN_TOL_RMS
+
+
+def _forces_rows(ctx, box, slabs):
+    """GPU accelerations of the given slabs, indexed by global particle row."""
+    db = ctx.box(box)
+    try:
+        out = np.zeros((box.n, db.record_width()), np.float32)
+        for s in slabs:
+            p0, p1 = db.slab_particles(s, s + 1)
+            out[p0:p1] = db.forces(s, s + 1)
+        return out
+    finally:
+        db.close()
+
+
+@pytest.mark.parametrize("name", ["uniform_cpd7", "clustered_cpd9", "sparse_cpd5"])
+@pytest.mark.parametrize("soft", [0, 1, 2, 3])
+def test_golden_parity(capi, oracle, name, soft):
+    import pathlib
+    path = pathlib.Path(__file__).parent / "golden" / f"{name}_{oracle.SOFTENING_NAMES[soft]}.npz"
+    box, soft_, eps, slabs, rows, acc = _golden(path)
+    with capi.Context(softening=soft_, eps=eps) as ctx:
+        a = _forces_rows(ctx, box, slabs)[rows]
+    _check_vs_ref(a, acc)
+    a64 = oracle.fp64_sinks(box, soft_, eps, rows)
+    rms, mx, _ = oracle.frac_errors(a[:, :3], a64)
+    assert rms <= FP64_RMS and mx <= FP64_MAX, (rms, mx)
+    assert np.all(a[:, 3] == 0)  # density channel off
+
+
+def test_uniform_64_plummer_full_box(capi, oracle, synth):
+    """64^3 uniform, cpd 17, Plummer eps = spacing/40: every slab against the
+    reference CPU restatement, and a sink sample against FP64."""
+    box = synth.config_uniform_64()
+    eps = synth.kernel_eps(0, synth.plummer_eps(64))
+    with capi.Context(softening=0, eps=eps) as ctx:
+        db = ctx.box(box)
+        a = db.forces(0, box.cpd)
+        t = ctx.last_timing()
+        pairs = db.pair_count()
+        db.close()
+    assert t.pairs == pairs == oracle.pair_count(box)
+    ref = np.zeros((box.n, 3), np.float32)
+    for s in range(box.cpd):
+        oracle.ref32_slab(box, 0, eps, s, acc=ref)
+    _check_vs_ref(a, ref)
+    sinks = np.sort(np.random.default_rng(0).choice(box.n, 3000, replace=False))
+    rms, mx, _ = oracle.frac_errors(a[sinks, :3], oracle.fp64_sinks(box, 0, eps, sinks))
+    assert rms <= FP64_RMS and mx <= FP64_MAX, (rms, mx)
+
+
+@pytest.mark.parametrize("acc_mode", [0, 1])
+def test_clustered_single_spline(capi, oracle, synth, acc_mode):
+    """Clustered 96^3 box, cpd 25 (occupancy 0 .. thousands): the heavy-tile
+    split path, the spline near branch, both accumulation modes."""
+    box = synth.clustered_box(96 ** 3, 25, seed=7, n_clumps=300)
+    assert box.counts.max() > 1000
+    eps = synth.kernel_eps(1, synth.plummer_eps(96))
+    with capi.Context(softening=1, eps=eps, accumulation=acc_mode) as ctx:
+        db = ctx.box(box)
+        a = db.forces()
+        db.close()
+    rng = np.random.default_rng(1)
+    sinks = np.sort(rng.choice(box.n, 2000, replace=False))
+    a64 = oracle.fp64_sinks(box, 1, eps, sinks)
+    rms, mx, _ = oracle.frac_errors(a[sinks, :3], a64)
+    assert rms <= FP64_RMS and mx <= FP64_MAX, (rms, mx)
+    cells = np.unique(np.searchsorted(box.cell_start, sinks, side="right") - 1)
+    ref = oracle.ref32_cells(box, 1, eps, cells)
+    _check_vs_ref(a[sinks], ref[sinks])
+
+
+def test_deterministic_and_range_consistent(capi, synth):
+    box = synth.clustered_box(40000, 13, seed=8, n_clumps=40)
+    eps = synth.kernel_eps(1, synth.plummer_eps(34))
+    with capi.Context(softening=1, eps=eps) as ctx:
+        db = ctx.box(box)
+        a1 = db.forces()
+        a2 = db.forces()
+        assert np.array_equal(a1.view(np.uint32), a2.view(np.uint32))
+        p0, p1 = db.slab_particles(4, 9)
+        b = db.forces(4, 9)
+        db.close()
+    np.testing.assert_allclose(b, a1[p0:p1], rtol=0, atol=1e-6 * np.abs(a1).max())
+
+
+def test_density_channel(capi, oracle, synth):
+    box = synth.clustered_box(30000, 11, seed=9, n_clumps=20)
+    eps = synth.kernel_eps(0, synth.plummer_eps(31))
+    b2 = float(np.float32((0.2 / 31) ** 2))
+    with capi.Context(softening=0, eps=eps, b2=b2) as ctx:
+        db = ctx.box(box)
+        a = db.forces()
+        db.close()
+    sinks = np.arange(0, box.n, 7)
+    w64 = oracle.fp64_density(box, b2, sinks)
+    np.testing.assert_allclose(a[sinks, 3], w64, rtol=1e-5, atol=1e-6 * b2)
+    assert (w64 > 0).mean() > 0.5
+    rms, mx, _ = oracle.frac_errors(a[sinks, :3], oracle.fp64_sinks(box, 0, eps, sinks))
+    assert rms <= FP64_RMS
+
+
+def test_radius_one_and_float3(capi, oracle, synth):
+    box = synth.uniform_box(20000, 9, seed=10)
+    eps = synth.kernel_eps(0, synth.plummer_eps(27))
+    with capi.Context(softening=0, eps=eps, near_field_radius=1, out_kind=capi.OUT_FLOAT3) as ctx:
+        db = ctx.box(box)
+        a = db.forces()
+        db.close()
+    assert a.shape == (box.n, 3)
+    sinks = np.arange(0, box.n, 5)
+    a64 = oracle.fp64_sinks(box, 0, eps, sinks, R=1)
+    rms, mx, _ = oracle.frac_errors(a[sinks], a64)
+    assert rms <= FP64_RMS, rms
+
+
+def test_forced_tile_shapes_agree(capi, synth):
+    box = synth.clustered_box(30000, 11, seed=11, n_clumps=25)
+    eps = synth.kernel_eps(1, synth.plummer_eps(31))
+    outs = []
+    for S in (1, 2, 4, 0):
+        with capi.Context(softening=1, eps=eps, sinks_per_lane=S) as ctx:
+            db = ctx.box(box)
+            outs.append(db.forces())
+            db.close()
+    for o in outs[1:]:
+        np.testing.assert_allclose(o, outs[0], rtol=0, atol=2e-6 * np.abs(outs[0]).max())
+
+
+def test_edge_cases(capi, oracle, synth):
+    # all particles in a single cell; most cells empty; minimum cpd for R=2
+    rng = np.random.default_rng(12)
+    n = 3000
+    cpd = 5
+    h = 1.0 / cpd
+    x = (rng.random(n, dtype=np.float32) - 0.5) * np.float32(0.999 * h)
+    y = (rng.random(n, dtype=np.float32) - 0.5) * np.float32(0.999 * h)
+    z = (rng.random(n, dtype=np.float32) - 0.5) * np.float32(0.999 * h)
+    cs = np.zeros(cpd ** 3 + 1, np.int64)
+    cs[63:] = n
+    box = synth.Box(cpd=cpd, x=x, y=y, z=z, cell_start=cs)
+    eps = synth.kernel_eps(1, 0.002)
+    with capi.Context(softening=1, eps=eps) as ctx:
+        db = ctx.box(box)
+        a = db.forces()
+        db.close()
+        # empty box
+        e = synth.Box(cpd=cpd, x=x[:0], y=y[:0], z=z[:0], cell_start=np.zeros(cpd ** 3 + 1, np.int64))
+        db = ctx.box(e)
+        assert db.forces().shape == (0, 4)
+        db.close()
+    sinks = np.arange(0, n, 3)
+    rms, mx, _ = oracle.frac_errors(a[sinks, :3], oracle.fp64_sinks(box, 1, eps, sinks))
+    assert rms <= FP64_RMS and mx <= FP64_MAX, (rms, mx)
+
+
+def test_errors_are_status_codes(capi, synth):
+    with pytest.raises(capi.NfError) as ei:
+        capi.Context(softening=7, eps=1.0)
+    assert ei.value.status == capi.NF_EINVAL
+    with pytest.raises(capi.NfError):
+        capi.Context(eps=float("inf"))
+    box = synth.uniform_box(1000, 5, seed=1)
+    with capi.Context(softening=0, eps=1e-6) as ctx:
+        db = ctx.box(box)
+        with pytest.raises(capi.NfError) as ei:
+            db.forces(3, 2)
+        assert ei.value.status == capi.NF_EINVAL
+        with pytest.raises(capi.NfError):
+            db.forces(0, 6)
+        db.close()

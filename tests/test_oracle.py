@@ -1,0 +1,111 @@
+"""The oracle, pinned against the reference's own CPU kernel (CPU only)."""
+import pathlib
+
+import numpy as np
+import pytest
+
+GOLDEN = pathlib.Path(__file__).resolve().parent / "golden"
+FIXTURES = sorted(GOLDEN.glob("*.npz"))
+
+
+class _Box:
+    def __init__(self, f):
+        self.cpd = int(f["cpd"])
+        self.x, self.y, self.z = f["x"], f["y"], f["z"]
+        self.cell_start = f["cell_start"]
+        self.n = self.x.size
+
+    def slab_range(self, s):
+        c2 = self.cpd ** 2
+        return int(self.cell_start[s * c2]), int(self.cell_start[(s + 1) * c2])
+
+
+def load_fixture(path):
+    f = np.load(path)
+    return _Box(f), int(f["softening"]), float(f["eps"]), list(f["slabs"]), f["rows"], f["acc"]
+
+
+def test_fixtures_present():
+    assert len(FIXTURES) == 12
+
+
+@pytest.mark.parametrize("path", FIXTURES, ids=lambda p: p.stem)
+def test_restatement_matches_golden_bitwise(oracle, path):
+    """nf_oracle.c reproduces singlestep/Direct/direct.cpp bit for bit."""
+    box, soft, eps, slabs, rows, acc = load_fixture(path)
+    out = np.zeros((box.n, 3), dtype=np.float32)
+    for s in slabs:
+        oracle.ref32_slab(box, soft, np.float32(eps), s, acc=out)
+    assert np.array_equal(out[rows].view(np.uint32), acc.view(np.uint32))
+
+
+@pytest.mark.parametrize("path", FIXTURES, ids=lambda p: p.stem)
+def test_fp64_oracle_agrees_with_reference(oracle, path):
+    """The FP64 sum agrees with the reference FP32 result to FP32 accuracy."""
+    box, soft, eps, slabs, rows, acc = load_fixture(path)
+    a64 = oracle.fp64_sinks(box, soft, eps, rows)
+    rms, mx, _ = oracle.frac_errors(acc, a64)
+    assert rms < 2e-6 and mx < 1e-4, (rms, mx)
+
+
+@pytest.mark.skipif(not (pathlib.Path(__file__).resolve().parents[1] / "oracle" / "_ref").exists(),
+                    reason="reference build not present")
+@pytest.mark.parametrize("soft", [0, 1, 2, 3])
+def test_restatement_matches_reference_build(oracle, synth, soft):
+    if not oracle.have_ref(soft):
+        pytest.skip("reference build not present")
+    box = synth.clustered_box(5000, 7, seed=99, n_clumps=5)
+    eps = synth.kernel_eps(soft, synth.plummer_eps(17))
+    a = oracle.ref32_slab(box, soft, eps, 2)
+    b = oracle.ref_slab(box, soft, eps, 2)
+    lo, hi = box.slab_range(2)
+    assert np.array_equal(a[lo:hi].view(np.uint32), b[lo:hi].view(np.uint32))
+
+
+def test_two_body_known_answer(oracle, synth):
+    """Two particles in one periodic box: a = -d / (r^2 + eps^2)^{3/2}."""
+    cpd = 5
+    h = 1.0 / cpd
+    x = np.array([0.01, -0.02], np.float32)
+    y = np.array([0.0, 0.015], np.float32)
+    z = np.array([0.0, 0.0], np.float32)
+    # both in the centre cell (2,2,2) -> id 62
+    cs = np.zeros(cpd ** 3 + 1, np.int64)
+    cs[63:] = 2
+    box = synth.Box(cpd=cpd, x=x, y=y, z=z, cell_start=cs)
+    eps2 = 1e-4
+    a = oracle.fp64_sinks(box, 0, eps2, np.array([0, 1]))
+    d = np.array([x[1] - x[0], y[1] - y[0], 0.0], np.float64)
+    g = (d @ d + np.float64(np.float32(eps2))) ** -1.5
+    np.testing.assert_allclose(a[0], -g * d, rtol=1e-12)
+    np.testing.assert_allclose(a[1], g * d, rtol=1e-12)
+    assert h > 0
+
+
+def test_lattice_symmetry(oracle, synth):
+    """A cubic lattice, one particle per cell at the centre: the 5x5x5 sum
+    cancels (the CheckForces idea, Tests/CheckForces/check_forces.py)."""
+    cpd = 7
+    n = cpd ** 3
+    cs = np.arange(n + 1, dtype=np.int64)
+    zero = np.zeros(n, np.float32)
+    box = synth.Box(cpd=cpd, x=zero, y=zero.copy(), z=zero.copy(), cell_start=cs)
+    for soft in (0, 1):
+        eps = synth.kernel_eps(soft, 0.01)
+        a64 = oracle.fp64_sinks(box, soft, eps, np.arange(0, n, 17))
+        assert np.abs(a64).max() < 1e-9
+        a32 = oracle.ref32_slab(box, soft, eps, 3)
+        lo, hi = box.slab_range(3)
+        scale = (1.0 / cpd) ** -2 if soft == 0 else 1.0
+        assert np.abs(a32[lo:hi]).max() < 1e-4 * scale
+
+
+def test_pair_count_formula(oracle, synth):
+    box = synth.clustered_box(4000, 9, seed=4, n_clumps=4)
+    counts = box.counts.reshape(9, 9, 9)
+    tot = 0
+    for dx in range(-2, 3):
+        for dy in range(-2, 3):
+            for dz in range(-2, 3):
+                tot += int((counts * np.roll(counts, (-dx, -dy, -dz), axis=(0, 1, 2))).sum())
+    assert oracle.pair_count(box) == tot
