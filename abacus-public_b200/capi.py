@@ -36,14 +36,14 @@ class Config(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("near_field_radius", ctypes.c_int),
                 ("softening", ctypes.c_int), ("eps", ctypes.c_float), ("b2", ctypes.c_float),
                 ("accumulation", ctypes.c_int), ("out_kind", ctypes.c_int),
-                ("sinks_per_lane", ctypes.c_int), ("warps_per_cta", ctypes.c_int)]
+                ("sinks_per_lane", ctypes.c_int), ("kernel_variant", ctypes.c_int)]
 
 
 class Timing(ctypes.Structure):
     _fields_ = [("kernel_ms", ctypes.c_float), ("coadd_ms", ctypes.c_float),
                 ("total_ms", ctypes.c_float), ("pairs", ctypes.c_uint64),
                 ("padded_pairs", ctypes.c_uint64), ("launches", ctypes.c_int),
-                ("items", ctypes.c_int)]
+                ("items", ctypes.c_int), ("variant", ctypes.c_int)]
 
 
 class GpuLimits(ctypes.Structure):
@@ -73,8 +73,65 @@ class SicDesc(ctypes.Structure):
                 ("bytes_from_device", ctypes.c_void_p)]
 
 
+CELLINFO_DTYPE = np.dtype([("startindex", "<u8"), ("startindex_with_ghost", "<u8"),
+                           ("count", "<i4"), ("active", "<i4"),
+                           ("mean_square_velocity", "<f4"), ("max_component_velocity", "<f4"),
+                           ("max_component_acceleration", "<f4")], align=True)
+
+
+class SlabView(ctypes.Structure):
+    _fields_ = [("posxyz", ctypes.c_void_p), ("nslab", ctypes.c_uint64),
+                ("cellinfo", ctypes.c_void_p), ("acc", ctypes.c_void_p)]
+
+
+class DriverParams(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("cpd", ctypes.c_int), ("np", ctypes.c_int64),
+                ("near_field_radius", ctypes.c_int), ("softening", ctypes.c_int),
+                ("softening_length", ctypes.c_double), ("density_kernel_rad2", ctypes.c_float),
+                ("direct_bpd", ctypes.c_int), ("mem_per_gpu_buffer_gb", ctypes.c_double),
+                ("max_ram_mb", ctypes.c_double), ("use_pinned_gpu_memory", ctypes.c_int),
+                ("accumulation", ctypes.c_int), ("out_kind", ctypes.c_int)]
+
+
+class DriverStats(ctypes.Structure):
+    _fields_ = [("direct_interactions", ctypes.c_uint64),
+                ("padded_direct_interactions", ctypes.c_uint64),
+                ("gdi_gpu", ctypes.c_double), ("gdi_padded_gpu", ctypes.c_double),
+                ("total_gb_to", ctypes.c_double), ("total_gb_from", ctypes.c_double),
+                ("total_sinks", ctypes.c_double), ("total_sources", ctypes.c_double),
+                ("total_padded_sinks", ctypes.c_double), ("total_padded_sources", ctypes.c_double),
+                ("mean_splits_per_slab", ctypes.c_double), ("max_nsplits", ctypes.c_int),
+                ("gpu_throughput_time", ctypes.c_double), ("calc_split_s", ctypes.c_double),
+                ("sic_construction_s", ctypes.c_double), ("sic_execute_s", ctypes.c_double),
+                ("finalize_s", ctypes.c_double), ("softening_length_internal", ctypes.c_double),
+                ("eps", ctypes.c_float), ("ngpu", ctypes.c_int), ("nbuffers", ctypes.c_int),
+                ("max_sink_blocks", ctypes.c_int), ("max_source_blocks", ctypes.c_int)]
+
+
+class SicSummary(ctypes.Structure):
+    _fields_ = [("nsinksets", ctypes.c_int), ("nsourcesets", ctypes.c_int),
+                ("nsinkblocks", ctypes.c_int), ("nsourceblocks", ctypes.c_int),
+                ("interaction_count", ctypes.c_int), ("direct_total", ctypes.c_uint64),
+                ("padded_direct_total", ctypes.c_uint64), ("sink_total", ctypes.c_uint64),
+                ("source_total", ctypes.c_uint64), ("padded_sink_total", ctypes.c_uint64),
+                ("padded_source_total", ctypes.c_uint64)]
+
+
 # Every symbol the header declares; the loader checks each one is exported.
 EXPORTS = {
+    "nf_driver_create": (ctypes.c_int, [ctypes.POINTER(DriverParams),
+                                        ctypes.POINTER(ctypes.c_void_p)]),
+    "nf_driver_set_slab": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int,
+                                          ctypes.POINTER(SlabView)]),
+    "nf_driver_execute_slab": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
+    "nf_driver_slab_done": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "nf_driver_finalize": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "nf_driver_aggregate_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(DriverStats)]),
+    "nf_driver_context": (ctypes.c_void_p, [ctypes.c_void_p]),
+    "nf_driver_destroy": (None, [ctypes.c_void_p]),
+    "nf_driver_plan_sic": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                          ctypes.c_int, ctypes.POINTER(SicSummary),
+                                          ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "nf_config_default": (None, [ctypes.POINTER(Config)]),
     "nf_init": (ctypes.c_int, [ctypes.POINTER(Config), ctypes.POINTER(ctypes.c_void_p)]),
     "nf_shutdown": (None, [ctypes.c_void_p]),
@@ -102,6 +159,10 @@ EXPORTS = {
                                          ctypes.c_int, ctypes.POINTER(ctypes.c_uint64)]),
     "nf_last_timing": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Timing)]),
     "nf_set_stream": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "nf_kernel_variant_count": (ctypes.c_int, []),
+    "nf_kernel_variant_name": (ctypes.c_char_p, [ctypes.c_int]),
+    "nf_box_tuning": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),
+                                     ctypes.POINTER(ctypes.c_float), ctypes.c_int]),
     "nf_measure_fp32_peak": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double,
                                             ctypes.POINTER(ctypes.c_double),
                                             ctypes.POINTER(ctypes.c_double)]),
@@ -232,6 +293,10 @@ class DeviceBox:
     def forces(self, lo: int = 0, hi: int | None = None, out: np.ndarray | None = None):
         """Accelerations of slabs [lo, hi) into host memory (float32[n, 3|4])."""
         hi = self.cpd if hi is None else hi
+        if not (0 <= lo < hi <= self.cpd):
+            # let the library report the bad range with its own status code
+            dummy = np.empty(1, dtype=np.float32)
+            check(lib().nf_box_forces(self.ctx.h, self.h, lo, hi, _ptr(dummy), 0), "nf_box_forces")
         p0, p1 = self.slab_particles(lo, hi)
         if out is None:
             out = np.empty((p1 - p0, self.record_width()), dtype=np.float32)
@@ -250,5 +315,122 @@ class DeviceBox:
               "nf_box_pair_count")
         return int(v.value)
 
+    def tuning(self) -> tuple[int, list[float]]:
+        v = ctypes.c_int(-1)
+        n = lib().nf_kernel_variant_count()
+        ms = (ctypes.c_float * n)()
+        check(lib().nf_box_tuning(self.h, ctypes.byref(v), ms, n), "nf_box_tuning")
+        return v.value, list(ms)
+
     def device_bytes(self) -> int:
         return int(lib().nf_box_device_bytes(self.h))
+
+
+class AbacusSlabs:
+    """A box laid out the way abacus holds it: one PosXYZ array
+    (X[n] | Y[n] | Z[n]), one cellinfo array (cpd*cpd cells, y-major) and one
+    AccSlab (accstruct per particle) per x-slab
+    (singlestep/DataModel/cellparticles.cpp:62-266)."""
+
+    def __init__(self, box, record_width: int = 4):
+        self.cpd = box.cpd
+        c2 = box.cpd * box.cpd
+        self.posxyz, self.cellinfo, self.acc, self.ranges = [], [], [], []
+        for s in range(box.cpd):
+            p0, p1 = int(box.cell_start[s * c2]), int(box.cell_start[(s + 1) * c2])
+            self.ranges.append((p0, p1))
+            self.posxyz.append(np.ascontiguousarray(
+                np.concatenate([box.x[p0:p1], box.y[p0:p1], box.z[p0:p1]]), dtype=np.float32))
+            ci = np.zeros(c2, dtype=CELLINFO_DTYPE)
+            starts = box.cell_start[s * c2:(s + 1) * c2] - p0
+            ci["startindex"] = starts
+            ci["startindex_with_ghost"] = starts
+            ci["count"] = np.diff(box.cell_start[s * c2:(s + 1) * c2 + 1])
+            ci["active"] = ci["count"]
+            self.cellinfo.append(ci)
+            self.acc.append(np.zeros((p1 - p0, record_width), dtype=np.float32))
+
+    def view(self, s: int) -> SlabView:
+        return SlabView(self.posxyz[s].ctypes.data, self.ranges[s][1] - self.ranges[s][0],
+                        self.cellinfo[s].ctypes.data, self.acc[s].ctypes.data)
+
+    def gather_acc(self, n: int) -> np.ndarray:
+        out = np.zeros((n, self.acc[0].shape[1]), dtype=np.float32)
+        for (p0, p1), a in zip(self.ranges, self.acc):
+            out[p0:p1] = a
+        return out
+
+
+class Driver:
+    """nf_driver: the NearFieldDriver mirror (device < 0: planner only)."""
+
+    def __init__(self, box, softening: int, softening_length: float, device: int = 0,
+                 near_field_radius: int = 2, direct_bpd: int = 3, mem_gb: float = 0.0,
+                 b2: float = 0.0, accumulation: int = ACC_COMPENSATED,
+                 out_kind: int = OUT_FLOAT4, use_pinned: int = -1):
+        p = DriverParams(device=device, cpd=box.cpd, np=box.n,
+                         near_field_radius=near_field_radius, softening=softening,
+                         softening_length=softening_length, density_kernel_rad2=b2,
+                         direct_bpd=direct_bpd, mem_per_gpu_buffer_gb=mem_gb, max_ram_mb=0.0,
+                         use_pinned_gpu_memory=use_pinned, accumulation=accumulation,
+                         out_kind=out_kind)
+        h = ctypes.c_void_p()
+        check(lib().nf_driver_create(ctypes.byref(p), ctypes.byref(h)), "nf_driver_create")
+        self.h = h
+        self.box = box
+        self.slabs = AbacusSlabs(box, 4 if out_kind == OUT_FLOAT4 else 3)
+        for s in range(box.cpd):
+            v = self.slabs.view(s)
+            check(lib().nf_driver_set_slab(self.h, s, ctypes.byref(v)), "nf_driver_set_slab")
+
+    def close(self):
+        if self.h:
+            lib().nf_driver_destroy(self.h)
+            self.h = None
+
+    def execute_slab(self, slab: int, blocking: int = 0):
+        check(lib().nf_driver_execute_slab(self.h, slab, blocking), "ExecuteSlab")
+
+    def slab_done(self, slab: int) -> int:
+        return lib().nf_driver_slab_done(self.h, slab)
+
+    def finalize(self, slab: int):
+        check(lib().nf_driver_finalize(self.h, slab), "Finalize")
+
+    def stats(self) -> DriverStats:
+        s = DriverStats()
+        check(lib().nf_driver_aggregate_stats(self.h, ctypes.byref(s)), "AggregateStats")
+        return s
+
+    def plan_sic(self, slab: int, jlow: int, jhigh: int):
+        s = SicSummary()
+        check(lib().nf_driver_plan_sic(self.h, slab, jlow, jhigh, ctypes.byref(s), None, None,
+                                       None), "plan")
+        a = np.zeros(s.nsinksets, np.int32)
+        b = np.zeros(s.nsinkblocks, np.int32)
+        c = np.zeros(s.nsourcesets, np.int32)
+        check(lib().nf_driver_plan_sic(self.h, slab, jlow, jhigh, ctypes.byref(s),
+                                       a.ctypes.data, b.ctypes.data, c.ctypes.data), "plan")
+        return s, a, b, c
+
+    def run_all(self, timeout_s: float = 600.0, blocking: int = 0):
+        """ExecuteSlab for every slab, then SlabDone polling and Finalize (the
+        NearForce -> Kick order of singlestep/Timestep/pipeline.cpp)."""
+        import time
+        for s in range(self.box.cpd):
+            self.execute_slab(s, blocking)
+        t0 = time.time()
+        pending = set(range(self.box.cpd))
+        while pending:
+            for s in list(pending):
+                d = self.slab_done(s)
+                if d < 0:
+                    raise NfError(NF_EDEVICE, f"slab {s} failed: {last_error()}")
+                if d == 1:
+                    self.finalize(s)
+                    pending.discard(s)
+            if pending:
+                if time.time() - t0 > timeout_s:
+                    raise NfError(NF_ETIMEDOUT, "slabs still in flight")
+                time.sleep(0.001)
+        return self.slabs.gather_acc(self.box.n)

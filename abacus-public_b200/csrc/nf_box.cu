@@ -128,47 +128,34 @@ __device__ __forceinline__ float4 load_src(const KParams &kp, const WarpSmem &ws
     return t;
 }
 
-template <int SOFT, bool DENS, int S, bool CHECK>
-__device__ __forceinline__ void chunk_fast(const float4 *buf, int m8, const float (&sx)[S],
-                                           const float (&sy)[S], const float (&sz)[S],
-                                           float (&cx)[S], float (&cy)[S], float (&cz)[S],
-                                           float (&cw)[S], float &mn, const PairConst &pc) {
+// One staged chunk (m_pad sources, a multiple of UNR) against the lane's S
+// sinks, accumulated straight into the running partials.  NEAR selects the
+// both-branch single-spline evaluation (source cells adjacent to the sink cell).
+template <int SOFT, bool DENS, int S, bool NEAR, int UNR>
+__device__ __forceinline__ void chunk_pairs(const float4 *buf, int m_pad, const float (&sx)[S],
+                                            const float (&sy)[S], const float (&sz)[S],
+                                            float (&px)[S], float (&py)[S], float (&pz)[S],
+                                            float (&pw)[S], const PairConst &pc) {
 #pragma unroll 1
-    for (int j = 0; j < m8; j += 8) {
+    for (int j = 0; j < m_pad; j += UNR) {
 #pragma unroll
-        for (int u = 0; u < 8; u++) {
+        for (int u = 0; u < UNR; u++) {
             float4 t = buf[j + u];
 #pragma unroll
             for (int s = 0; s < S; s++) {
                 float dx = t.x - sx[s], dy = t.y - sy[s], dz = t.z - sz[s];
-                float r2;
-                float g = pair_g_fast<SOFT>(dx, dy, dz, pc, r2);
-                if (CHECK) mn = fminf(mn, r2);
-                cx[s] = fmaf(-g, dx, cx[s]);
-                cy[s] = fmaf(-g, dy, cy[s]);
-                cz[s] = fmaf(-g, dz, cz[s]);
-                if (DENS) cw[s] += dens_term(dx, dy, dz, pc.b2);
+                float g;
+                if (NEAR) {
+                    g = spline_g_both(dx, dy, dz, pc);
+                } else {
+                    float r2;
+                    g = pair_g_fast<SOFT>(dx, dy, dz, pc, r2);
+                }
+                px[s] = fmaf(-g, dx, px[s]);
+                py[s] = fmaf(-g, dy, py[s]);
+                pz[s] = fmaf(-g, dz, pz[s]);
+                if (DENS) pw[s] += dens_term(dx, dy, dz, pc.b2);
             }
-        }
-    }
-}
-
-template <bool DENS, int S>
-__device__ __forceinline__ void chunk_spline_exact(const float4 *buf, int m8, const float (&sx)[S],
-                                                const float (&sy)[S], const float (&sz)[S],
-                                                float (&cx)[S], float (&cy)[S], float (&cz)[S],
-                                                float (&cw)[S], const PairConst &pc) {
-#pragma unroll 1
-    for (int j = 0; j < m8; j++) {
-        float4 t = buf[j];
-#pragma unroll
-        for (int s = 0; s < S; s++) {
-            float dx = t.x - sx[s], dy = t.y - sy[s], dz = t.z - sz[s];
-            float g = spline_g_exact(dx, dy, dz, pc);
-            cx[s] = fmaf(-g, dx, cx[s]);
-            cy[s] = fmaf(-g, dy, cy[s]);
-            cz[s] = fmaf(-g, dz, cz[s]);
-            if (DENS) cw[s] += dens_term(dx, dy, dz, pc.b2);
         }
     }
 }
@@ -178,40 +165,52 @@ struct CombSmem {
     double v[WARPS_PER_CTA][4][TILE_MAX];
 };
 
-template <int SOFT, bool DENS, int S>
+// Particle index and pencil slot of sink i of the tile's pencil.
+__device__ __forceinline__ int64_t sink_particle(const WarpSmem &ws, int i, int &a) {
+    a = 0;
+    while (i >= ws.spre[a + 1]) a++;
+    return ws.sstart[a] + (i - ws.spre[a]);
+}
+
+template <int S>
+__device__ __forceinline__ void fold(float (&h)[S], float (&l)[S], float (&p)[S], bool plain) {
+#pragma unroll
+    for (int s = 0; s < S; s++) {
+        if (plain) {
+            h[s] += p[s];
+        } else {
+            float e;
+            two_sum(h[s], p[s], h[s], e);
+            l[s] += e;
+        }
+        p[s] = 0.f;
+    }
+}
+
+template <int SOFT, bool DENS, int S, int UNR>
 __device__ void run_tile(const KParams &kp, WarpSmem &ws, const Item &it, int lane,
                          CombSmem *comb, int wslot) {
     const int NC = DENS ? 4 : 3;
     float sx[S], sy[S], sz[S];
-    int64_t sp[S];
-    int sa[S];
 #pragma unroll
     for (int s = 0; s < S; s++) {
         int j = s * 32 + lane;
-        sp[s] = -1;
-        sa[s] = 0;
-        sx[s] = -1e18f;
-        sy[s] = -1e18f;
-        sz[s] = -1e18f;
+        sx[s] = sy[s] = sz[s] = -1e18f;  // idle lane: far from every source
         if (j < it.nsink) {
-            int i = it.sink_begin + j;
-            int a = 0;
-            while (i >= ws.spre[a + 1]) a++;
-            int64_t p = ws.sstart[a] + (i - ws.spre[a]);
+            int a;
+            int64_t p = sink_particle(ws, it.sink_begin + j, a);
             float4 q = __ldg(&kp.pos[p]);
             sx[s] = q.x;
             sy[s] = q.y;
             sz[s] = q.z + kp.zshift[a];
-            sp[s] = p;
-            sa[s] = a;
         }
     }
-    float hx[S], hy[S], hz[S], lx[S], ly[S], lz[S], px[S], py[S], pz[S], hw[S];
+    float hx[S], hy[S], hz[S], lx[S], ly[S], lz[S], px[S], py[S], pz[S], pw[S];
 #pragma unroll
-    for (int s = 0; s < S; s++) {
-        hx[s] = hy[s] = hz[s] = lx[s] = ly[s] = lz[s] = px[s] = py[s] = pz[s] = hw[s] = 0.f;
-    }
+    for (int s = 0; s < S; s++)
+        hx[s] = hy[s] = hz[s] = lx[s] = ly[s] = lz[s] = px[s] = py[s] = pz[s] = pw[s] = 0.f;
     const int inner_begin = ws.cpre[kp.n_outer];
+    const bool plain = kp.plain;
     int k = 0;
     int base = it.src_begin;
     float4 pre = load_src(kp, ws, base + lane, it.src_end, k);
@@ -222,103 +221,63 @@ __device__ void run_tile(const KParams &kp, WarpSmem &ws, const Item &it, int la
         __syncwarp();
         if (base + 32 < it.src_end) pre = load_src(kp, ws, base + 32 + lane, it.src_end, k);
         int m = min(32, it.src_end - base);
-        int m8 = (m + 7) & ~7;
-        float cx[S], cy[S], cz[S], cw[S];
-#pragma unroll
-        for (int s = 0; s < S; s++) cx[s] = cy[s] = cz[s] = cw[s] = 0.f;
-        float mn = 3.0e38f;
-        if (SOFT == SOFT_SINGLE_SPLINE && base + 32 > inner_begin) {
-            chunk_fast<SOFT, DENS, S, true>(ws.buf, m8, sx, sy, sz, cx, cy, cz, cw, mn, kp.pc);
-            if (__any_sync(FULL, mn < kp.pc.near_thr)) {
-#pragma unroll
-                for (int s = 0; s < S; s++) cx[s] = cy[s] = cz[s] = cw[s] = 0.f;
-                chunk_spline_exact<DENS, S>(ws.buf, m8, sx, sy, sz, cx, cy, cz, cw, kp.pc);
-            }
-        } else {
-            chunk_fast<SOFT, DENS, S, false>(ws.buf, m8, sx, sy, sz, cx, cy, cz, cw, mn, kp.pc);
-        }
-#pragma unroll
-        for (int s = 0; s < S; s++) {
-            px[s] += cx[s];
-            py[s] += cy[s];
-            pz[s] += cz[s];
-            if (DENS) hw[s] += cw[s];
-        }
-        if (++nchunk == 2) {
+        int m_pad = (m + UNR - 1) / UNR * UNR;
+        if (SOFT == SOFT_SINGLE_SPLINE && base + 32 > inner_begin)
+            chunk_pairs<SOFT, DENS, S, true, UNR>(ws.buf, m_pad, sx, sy, sz, px, py, pz, pw, kp.pc);
+        else
+            chunk_pairs<SOFT, DENS, S, false, UNR>(ws.buf, m_pad, sx, sy, sz, px, py, pz, pw, kp.pc);
+        if (++nchunk == 2) {  // fold every 64 sources
             nchunk = 0;
-#pragma unroll
-            for (int s = 0; s < S; s++) {
-                if (kp.plain) {
-                    hx[s] += px[s];
-                    hy[s] += py[s];
-                    hz[s] += pz[s];
-                } else {
-                    float e;
-                    two_sum(hx[s], px[s], hx[s], e);
-                    lx[s] += e;
-                    two_sum(hy[s], py[s], hy[s], e);
-                    ly[s] += e;
-                    two_sum(hz[s], pz[s], hz[s], e);
-                    lz[s] += e;
-                }
-                px[s] = py[s] = pz[s] = 0.f;
-            }
+            fold<S>(hx, lx, px, plain);
+            fold<S>(hy, ly, py, plain);
+            fold<S>(hz, lz, pz, plain);
         }
     }
+    fold<S>(hx, lx, px, plain);
+    fold<S>(hy, ly, py, plain);
+    fold<S>(hz, lz, pz, plain);
 #pragma unroll
     for (int s = 0; s < S; s++) {
-        if (kp.plain) {
-            hx[s] += px[s];
-            hy[s] += py[s];
-            hz[s] += pz[s];
-        } else {
-            float e;
-            two_sum(hx[s], px[s], hx[s], e);
-            lx[s] += e;
-            two_sum(hy[s], py[s], hy[s], e);
-            ly[s] += e;
-            two_sum(hz[s], pz[s], hz[s], e);
-            lz[s] += e;
-        }
-    }
-#pragma unroll
-    for (int s = 0; s < S; s++) {
+        int j = s * 32 + lane;
+        if (j >= it.nsink) continue;
         double vx = (double)hx[s] + (double)lx[s];
         double vy = (double)hy[s] + (double)ly[s];
         double vz = (double)hz[s] + (double)lz[s];
-        int j = s * 32 + lane;
         if (comb) {
-            if (j < it.nsink) {
-                comb->v[wslot][0][j] = vx;
-                comb->v[wslot][1][j] = vy;
-                comb->v[wslot][2][j] = vz;
-                if (DENS) comb->v[wslot][3][j] = (double)hw[s];
-            }
-        } else if (sp[s] >= 0) {
-            int64_t idx = sp[s] - kp.p0;
-            double *base_p = kp.part + (int64_t)sa[s] * NC * kp.n_range + idx;
-            base_p[0] = vx;
-            base_p[kp.n_range] = vy;
-            base_p[2 * kp.n_range] = vz;
-            if (DENS) base_p[3 * kp.n_range] = (double)hw[s];
+            comb->v[wslot][0][j] = vx;
+            comb->v[wslot][1][j] = vy;
+            comb->v[wslot][2][j] = vz;
+            if (DENS) comb->v[wslot][3][j] = (double)pw[s];
+        } else {
+            int a;
+            int64_t idx = sink_particle(ws, it.sink_begin + j, a) - kp.p0;
+            double *bp = kp.part + (int64_t)a * NC * kp.n_range + idx;
+            bp[0] = vx;
+            bp[kp.n_range] = vy;
+            bp[2 * kp.n_range] = vz;
+            if (DENS) bp[3 * kp.n_range] = (double)pw[s];
         }
     }
 }
 
-template <int SOFT, bool DENS>
+template <int SOFT, bool DENS, int SMAX, int UNR>
 __device__ __forceinline__ void dispatch_tile(const KParams &kp, WarpSmem &ws, const Item &it,
                                               int lane, CombSmem *comb, int wslot) {
     setup_tables(kp, it, ws, lane);
     if (it.S == 1)
-        run_tile<SOFT, DENS, 1>(kp, ws, it, lane, comb, wslot);
-    else if (it.S == 2)
-        run_tile<SOFT, DENS, 2>(kp, ws, it, lane, comb, wslot);
+        run_tile<SOFT, DENS, 1, UNR>(kp, ws, it, lane, comb, wslot);
+    else if (SMAX == 2 || it.S == 2)
+        run_tile<SOFT, DENS, 2, UNR>(kp, ws, it, lane, comb, wslot);
     else
-        run_tile<SOFT, DENS, 4>(kp, ws, it, lane, comb, wslot);
+        run_tile<SOFT, DENS, (SMAX >= 4 ? 4 : 2), UNR>(kp, ws, it, lane, comb, wslot);
 }
 
-template <int SOFT, bool DENS>
-__global__ void __launch_bounds__(WARPS_PER_CTA * 32, 2) pencil_kernel(KParams kp) {
+// The persistent pencil kernel.  Shape knobs (chosen by the autotuner):
+//   SMAX  largest tile 32*SMAX sinks (S = sinks per lane in {1, 2, SMAX})
+//   UNR   sources per unrolled step
+//   MINB  CTAs per SM the register allocation must leave room for
+template <int SOFT, bool DENS, int SMAX, int UNR, int MINB>
+__global__ void __launch_bounds__(WARPS_PER_CTA * 32, MINB) pencil_kernel(KParams kp) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     WarpSmem *wsm = reinterpret_cast<WarpSmem *>(smem_raw);
     CombSmem *comb = reinterpret_cast<CombSmem *>(smem_raw + sizeof(WarpSmem) * WARPS_PER_CTA);
@@ -333,16 +292,13 @@ __global__ void __launch_bounds__(WARPS_PER_CTA * 32, 2) pencil_kernel(KParams k
         __syncthreads();
         if (g >= kp.n_heavy_groups) break;
         Item it = kp.heavy[(int64_t)g * WARPS_PER_CTA + warp];
-        dispatch_tile<SOFT, DENS>(kp, wsm[warp], it, lane, comb, warp);
+        dispatch_tile<SOFT, DENS, SMAX, UNR>(kp, wsm[warp], it, lane, comb, warp);
         __syncthreads();
         // warp 0's tables describe the (common) sink tile
         const WarpSmem &w0 = wsm[0];
         for (int j = threadIdx.x; j < it.nsink; j += blockDim.x) {
-            int i = it.sink_begin + j;
-            int a = 0;
-            while (i >= w0.spre[a + 1]) a++;
-            int64_t p = w0.sstart[a] + (i - w0.spre[a]);
-            int64_t idx = p - kp.p0;
+            int a;
+            int64_t idx = sink_particle(w0, it.sink_begin + j, a) - kp.p0;
             double *bp = kp.part + (int64_t)a * NC * kp.n_range + idx;
 #pragma unroll
             for (int c = 0; c < NC; c++) {
@@ -361,7 +317,7 @@ __global__ void __launch_bounds__(WARPS_PER_CTA * 32, 2) pencil_kernel(KParams k
         i = __shfl_sync(FULL, i, 0);
         if (i >= kp.n_light) break;
         Item it = kp.light[i];
-        dispatch_tile<SOFT, DENS>(kp, wsm[warp], it, lane, nullptr, 0);
+        dispatch_tile<SOFT, DENS, SMAX, UNR>(kp, wsm[warp], it, lane, nullptr, 0);
     }
 }
 
@@ -399,15 +355,51 @@ __global__ void pack_positions(const float *__restrict__ x, const float *__restr
 
 typedef void (*KernelFn)(KParams);
 
-static KernelFn pick_kernel(int soft, bool dens) {
+// Kernel shapes the autotuner chooses among (tunable for the Plummer and
+// single-spline kernels without the density channel; the other kernels run
+// shape 0).
+struct Variant {
+    int smax, unr, minb;
+    const char *name;
+};
+static const Variant VARIANTS[] = {
+    {4, 8, 2, "sinks/lane<=4 unroll 8, 2 CTAs/SM"},
+    {4, 4, 2, "sinks/lane<=4 unroll 4, 2 CTAs/SM"},
+    {4, 4, 3, "sinks/lane<=4 unroll 4, 3 CTAs/SM"},
+    {2, 8, 3, "sinks/lane<=2 unroll 8, 3 CTAs/SM"},
+    {2, 4, 4, "sinks/lane<=2 unroll 4, 4 CTAs/SM"},
+};
+static constexpr int NVARIANTS = sizeof(VARIANTS) / sizeof(VARIANTS[0]);
+
+template <int SOFT, bool DENS>
+static KernelFn variant_kernel(int v) {
+    switch (v) {
+    case 1: return pencil_kernel<SOFT, DENS, 4, 4, 2>;
+    case 2: return pencil_kernel<SOFT, DENS, 4, 4, 3>;
+    case 3: return pencil_kernel<SOFT, DENS, 2, 8, 3>;
+    case 4: return pencil_kernel<SOFT, DENS, 2, 4, 4>;
+    default: return pencil_kernel<SOFT, DENS, 4, 8, 2>;
+    }
+}
+
+static bool tunable(int soft, bool dens) {
+    return !dens && (soft == SOFT_PLUMMER || soft == SOFT_SINGLE_SPLINE);
+}
+
+static KernelFn pick_kernel(int soft, bool dens, int v) {
+    if (!tunable(soft, dens)) v = 0;
     switch (soft) {
-    case SOFT_PLUMMER: return dens ? pencil_kernel<SOFT_PLUMMER, true> : pencil_kernel<SOFT_PLUMMER, false>;
+    case SOFT_PLUMMER:
+        return dens ? pencil_kernel<SOFT_PLUMMER, true, 4, 8, 2> : variant_kernel<SOFT_PLUMMER, false>(v);
     case SOFT_SINGLE_SPLINE:
-        return dens ? pencil_kernel<SOFT_SINGLE_SPLINE, true> : pencil_kernel<SOFT_SINGLE_SPLINE, false>;
+        return dens ? pencil_kernel<SOFT_SINGLE_SPLINE, true, 4, 8, 2>
+                    : variant_kernel<SOFT_SINGLE_SPLINE, false>(v);
     case SOFT_CUBIC_SPLINE:
-        return dens ? pencil_kernel<SOFT_CUBIC_SPLINE, true> : pencil_kernel<SOFT_CUBIC_SPLINE, false>;
+        return dens ? pencil_kernel<SOFT_CUBIC_SPLINE, true, 4, 8, 2>
+                    : pencil_kernel<SOFT_CUBIC_SPLINE, false, 4, 8, 2>;
     default:
-        return dens ? pencil_kernel<SOFT_CUBIC_PLUMMER, true> : pencil_kernel<SOFT_CUBIC_PLUMMER, false>;
+        return dens ? pencil_kernel<SOFT_CUBIC_PLUMMER, true, 4, 8, 2>
+                    : pencil_kernel<SOFT_CUBIC_PLUMMER, false, 4, 8, 2>;
     }
 }
 
@@ -445,7 +437,7 @@ struct HostTile {
     double cost;
 };
 
-static nf_status build_plan(nf_ctx *ctx, nf_box *box, int lo, int hi, Plan &pl) {
+static nf_status build_plan(nf_ctx *ctx, nf_box *box, int lo, int hi, int variant, Plan &pl) {
     const int cpd = box->cpd, R = ctx->cfg.near_field_radius, W = 2 * R + 1;
     const auto &cs = box->cell_start;
     auto count = [&](int x, int y, int z) -> int64_t {
@@ -454,6 +446,9 @@ static nf_status build_plan(nf_ctx *ctx, nf_box *box, int lo, int hi, Plan &pl) 
     };
     pl.lo = lo;
     pl.hi = hi;
+    pl.variant = variant;
+    const int smax = VARIANTS[variant].smax;
+    const int unr = VARIANTS[variant].unr;
     pl.p0 = cs[(int64_t)lo * cpd * cpd];
     pl.n_range = cs[(int64_t)hi * cpd * cpd] - pl.p0;
     std::vector<HostTile> tiles;
@@ -480,13 +475,13 @@ static nf_status build_plan(nf_ctx *ctx, nf_box *box, int lo, int hi, Plan &pl) 
                     int64_t rem = np_ - done;
                     int S;
                     if (forced_S)
-                        S = forced_S;
+                        S = std::min(forced_S, smax);
                     else
-                        S = rem <= 32 ? 1 : (rem <= 64 ? 2 : 4);
+                        S = rem <= 32 ? 1 : (rem <= 64 || smax == 2 ? 2 : 4);
                     int take = (int)std::min<int64_t>(rem, 32 * S);
                     HostTile t;
                     t.it = Item{pencil, (int)done, take, S, 0, (int)M, 0, 0};
-                    int64_t Mpad = ((M + 7) / 8) * 8;
+                    int64_t Mpad = (M / 32) * 32 + ((M % 32) + unr - 1) / unr * unr;
                     t.cost = (double)(32 * S) * (double)Mpad + 2000.0 * S;
                     pairs += (uint64_t)take * (uint64_t)M;
                     padded += (uint64_t)(32 * S) * (uint64_t)Mpad;
@@ -498,7 +493,7 @@ static nf_status build_plan(nf_ctx *ctx, nf_box *box, int lo, int hi, Plan &pl) 
     pl.pairs = pairs;
     pl.padded_pairs = padded;
     // occupancy-derived persistent grid
-    KernelFn fn = pick_kernel(ctx->cfg.softening, ctx->cfg.b2 > 0.f);
+    KernelFn fn = pick_kernel(ctx->cfg.softening, ctx->cfg.b2 > 0.f, variant);
     int per_sm = 0;
     NF_CUDA(cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)kernel_smem()));
@@ -565,33 +560,36 @@ static void free_plan(Plan &pl) {
     pl = Plan{};
 }
 
-static KParams make_params(nf_ctx *ctx, nf_box *box, const Plan &pl) {
+static KParams params_from(nf_ctx *ctx, const EngineLaunch &L) {
     KParams kp;
     memset(&kp, 0, sizeof(kp));
     const nf_config &cfg = ctx->cfg;
     const int R = cfg.near_field_radius;
-    kp.pos = box->d_pos;
-    kp.cs = box->d_cs;
-    kp.cpd = box->cpd;
+    kp.pos = L.pos;
+    kp.cs = L.cs;
+    kp.cpd = L.cpd;
     kp.R = R;
-    kp.heavy = pl.d_heavy;
-    kp.n_heavy_groups = pl.n_heavy_groups;
-    kp.light = pl.d_light;
-    kp.n_light = pl.n_light;
-    kp.counters = pl.d_counters;
-    kp.part = box->d_part;
-    kp.p0 = pl.p0;
-    kp.n_range = pl.n_range;
+    kp.heavy = L.heavy;
+    kp.n_heavy_groups = L.n_heavy_groups;
+    kp.light = L.light;
+    kp.n_light = L.n_light;
+    kp.counters = L.counters;
+    kp.part = L.part;
+    kp.p0 = L.p0;
+    kp.n_range = L.n_range;
     kp.nc = cfg.b2 > 0.f ? 4 : 3;
     kp.plain = cfg.accumulation == NF_ACC_PLAIN;
     kp.pc.eps = cfg.eps;
     kp.pc.b2 = cfg.b2;
     if (cfg.softening == SOFT_SINGLE_SPLINE) {
-        double e2 = 1.0 / (double)cfg.eps;  // eps_int^2
-        kp.pc.near_thr = (float)(e2 * 1.0001);
-        kp.pc.inv_eps3 = (float)pow((double)cfg.eps, 1.5);
+        double ie2 = (double)cfg.eps;  // eps_int^-2
+        kp.pc.near_thr = (float)(1.0 / ie2);
+        kp.pc.inv_eps3 = (float)pow(ie2, 1.5);
+        kp.pc.c1 = (float)(-15.0 * ie2 * ie2);
+        kp.pc.c2 = (float)(6.0 * pow(ie2, 2.5));
+        kp.pc.c3 = (float)(10.0 * pow(ie2, 1.5));
     }
-    double h = 1.0 / (double)box->cpd;
+    double h = 1.0 / (double)L.cpd;
     for (int a = 0; a < 2 * R + 1; a++) {
         kp.zshift[a] = (float)((a - R) * h);
         kp.xyshift[a] = (float)((a - R) * h);
@@ -600,15 +598,80 @@ static KParams make_params(nf_ctx *ctx, nf_box *box, const Plan &pl) {
     return kp;
 }
 
+static KParams make_params(nf_ctx *ctx, nf_box *box, const Plan &pl) {
+    EngineLaunch L;
+    L.pos = box->d_pos;
+    L.cs = box->d_cs;
+    L.cpd = box->cpd;
+    L.heavy = pl.d_heavy;
+    L.n_heavy_groups = pl.n_heavy_groups;
+    L.light = pl.d_light;
+    L.n_light = pl.n_light;
+    L.counters = pl.d_counters;
+    L.part = box->d_part;
+    L.p0 = pl.p0;
+    L.n_range = pl.n_range;
+    L.variant = pl.variant;
+    return params_from(ctx, L);
+}
+
 static double output_scale(const nf_config &cfg) {
     if (cfg.softening == SOFT_SINGLE_SPLINE) return pow((double)cfg.eps, -1.5);  // eps_int^3
     return 1.0;
 }
 
+int engine_variant_smax(int variant) { return VARIANTS[variant].smax; }
+// The plain drop-in runs the reference's block shape: 64-sink tiles.
+int engine_plain_variant() { return 3; }
+
+int engine_grid(nf_ctx *ctx, int variant) {
+    KernelFn fn = pick_kernel(ctx->cfg.softening, ctx->cfg.b2 > 0.f, variant);
+    int per_sm = 0;
+    if (cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)kernel_smem()) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)fn,
+                                                      WARPS_PER_CTA * 32, kernel_smem()) !=
+            cudaSuccess) {
+        cudaGetLastError();
+        per_sm = 1;
+    }
+    return ctx->sms * std::max(per_sm, 1);
+}
+
+nf_status engine_launch(nf_ctx *ctx, const EngineLaunch &L, double, cudaStream_t st) {
+    if (L.n_heavy_groups + L.n_light == 0) return NF_OK;
+    KParams kp = params_from(ctx, L);
+    KernelFn fn = pick_kernel(ctx->cfg.softening, ctx->cfg.b2 > 0.f, L.variant);
+    NF_CUDA(cudaMemsetAsync(L.counters, 0, 2 * sizeof(int), st));
+    int grid = L.grid > 0 ? L.grid : engine_grid(ctx, L.variant);
+    void *args[] = {&kp};
+    NF_CUDA(cudaLaunchKernel((const void *)fn, dim3(grid), dim3(WARPS_PER_CTA * 32), args,
+                             kernel_smem(), st));
+    return NF_OK;
+}
+
+nf_status engine_coadd(nf_ctx *ctx, const double *part, int64_t n, void *out, cudaStream_t st) {
+    if (n <= 0) return NF_OK;
+    const nf_config &cfg = ctx->cfg;
+    coadd_kernel<<<ctx->sms * 8, 256, 0, st>>>(part, n, 2 * cfg.near_field_radius + 1,
+                                              cfg.b2 > 0.f ? 4 : 3, output_scale(cfg),
+                                              cfg.out_kind, out);
+    NF_CUDA(cudaGetLastError());
+    return NF_OK;
+}
+
+nf_status engine_pack(nf_ctx *ctx, const float *x, const float *y, const float *z, int64_t n,
+                      float4 *out, cudaStream_t st) {
+    if (n <= 0) return NF_OK;
+    pack_positions<<<ctx->sms * 8, 256, 0, st>>>(x, y, z, n, out);
+    NF_CUDA(cudaGetLastError());
+    return NF_OK;
+}
+
 static nf_status enqueue_forces(nf_ctx *ctx, nf_box *box, Plan &pl, cudaStream_t st) {
     const nf_config &cfg = ctx->cfg;
     KParams kp = make_params(ctx, box, pl);
-    KernelFn fn = pick_kernel(cfg.softening, cfg.b2 > 0.f);
+    KernelFn fn = pick_kernel(cfg.softening, cfg.b2 > 0.f, pl.variant);
     NF_CUDA(cudaMemsetAsync(pl.d_counters, 0, 2 * sizeof(int), st));
     NF_CUDA(cudaEventRecordWithFlags(ctx->ev[0], st, cudaEventRecordExternal));
     if (pl.n_heavy_groups + pl.n_light > 0) {
@@ -761,6 +824,88 @@ extern "C" nf_status nf_box_pair_count(nf_ctx *ctx, const nf_box *box, int lo, i
     return NF_OK;
 }
 
+// Partial scratch: (2R+1) slots x nc components x n_range doubles, shared by
+// the box's plans (grown on demand; cached graphs that refer to the old
+// buffer are dropped).
+static nf_status ensure_scratch(nf_ctx *ctx, nf_box *box, int64_t n_range) {
+    int nc = ctx->cfg.b2 > 0.f ? 4 : 3;
+    size_t need = (size_t)(2 * ctx->cfg.near_field_radius + 1) * nc * (size_t)n_range * sizeof(double);
+    if (need <= box->part_bytes) return NF_OK;
+    cudaFree(box->d_part);
+    box->d_part = nullptr;
+    box->part_bytes = 0;
+    for (auto &kv : box->plans)
+        if (kv.second->graph) {
+            cudaGraphExecDestroy(kv.second->graph);
+            kv.second->graph = nullptr;
+        }
+    if (cudaMalloc(&box->d_part, need) != cudaSuccess) {
+        cudaGetLastError();
+        set_error("nf_box_forces: cannot allocate partial scratch");
+        return NF_ENOMEM;
+    }
+    box->part_bytes = need;
+    return NF_OK;
+}
+
+static nf_status new_plan(nf_ctx *ctx, nf_box *box, int lo, int hi, int variant,
+                          std::unique_ptr<Plan> &out) {
+    std::unique_ptr<Plan> pl(new Plan);
+    nf_status st = build_plan(ctx, box, lo, hi, variant, *pl);
+    if (st == NF_OK) st = ensure_scratch(ctx, box, pl->n_range);
+    if (st != NF_OK) {
+        free_plan(*pl);
+        return st;
+    }
+    out = std::move(pl);
+    return NF_OK;
+}
+
+// Device time of one launch of a plan's pencil kernel (no co-add).
+static nf_status time_pencil(nf_ctx *ctx, nf_box *box, Plan &pl, float *ms) {
+    cudaStream_t st = ctx->stream;
+    KParams kp = make_params(ctx, box, pl);
+    KernelFn fn = pick_kernel(ctx->cfg.softening, ctx->cfg.b2 > 0.f, pl.variant);
+    NF_CUDA(cudaMemsetAsync(pl.d_counters, 0, 2 * sizeof(int), st));
+    NF_CUDA(cudaEventRecord(ctx->ev[0], st));
+    if (pl.n_heavy_groups + pl.n_light > 0) {
+        void *args[] = {&kp};
+        NF_CUDA(cudaLaunchKernel((const void *)fn, dim3(pl.grid), dim3(WARPS_PER_CTA * 32), args,
+                                 kernel_smem(), st));
+    }
+    NF_CUDA(cudaEventRecord(ctx->ev[1], st));
+    NF_CUDA(cudaEventSynchronize(ctx->ev[1]));
+    NF_CUDA(cudaEventElapsedTime(ms, ctx->ev[0], ctx->ev[1]));
+    return NF_OK;
+}
+
+// The autotuner: run every candidate kernel shape on the requested slab
+// range (one warm-up launch, one timed launch each) and keep the fastest
+// for the box.
+static nf_status autotune(nf_ctx *ctx, nf_box *box, int lo, int hi) {
+    const bool tun = tunable(ctx->cfg.softening, ctx->cfg.b2 > 0.f);
+    const int nv = tun ? NVARIANTS : 1;
+    int best = 0;
+    float best_ms = 3.0e38f;
+    for (int v = 0; v < nv; v++) {
+        std::unique_ptr<Plan> pl;
+        nf_status st = new_plan(ctx, box, lo, hi, v, pl);
+        if (st != NF_OK) return st;
+        float ms = 0;
+        st = time_pencil(ctx, box, *pl, &ms);
+        if (st == NF_OK) st = time_pencil(ctx, box, *pl, &ms);
+        free_plan(*pl);
+        if (st != NF_OK) return st;
+        box->tune_ms[v] = ms;
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = v;
+        }
+    }
+    box->variant = best;
+    return NF_OK;
+}
+
 static nf_status get_plan(nf_ctx *ctx, nf_box *box, int lo, int hi, Plan **out) {
     auto key = std::make_pair(lo, hi);
     auto it = box->plans.find(key);
@@ -768,35 +913,35 @@ static nf_status get_plan(nf_ctx *ctx, nf_box *box, int lo, int hi, Plan **out) 
         *out = it->second.get();
         return NF_OK;
     }
-    std::unique_ptr<Plan> pl(new Plan);
-    nf_status st = build_plan(ctx, box, lo, hi, *pl);
-    if (st != NF_OK) {
-        free_plan(*pl);
-        return st;
-    }
-    // partial scratch: (2R+1) slots x nc components x n_range doubles
-    int nc = ctx->cfg.b2 > 0.f ? 4 : 3;
-    size_t need = (size_t)(2 * ctx->cfg.near_field_radius + 1) * nc * (size_t)pl->n_range * sizeof(double);
-    if (need > box->part_bytes) {
-        cudaFree(box->d_part);
-        box->d_part = nullptr;
-        box->part_bytes = 0;
-        // every cached graph refers to the old scratch: drop them
-        for (auto &kv : box->plans)
-            if (kv.second->graph) {
-                cudaGraphExecDestroy(kv.second->graph);
-                kv.second->graph = nullptr;
-            }
-        if (cudaMalloc(&box->d_part, need) != cudaSuccess) {
-            cudaGetLastError();
-            free_plan(*pl);
-            set_error("nf_box_forces: cannot allocate partial scratch");
-            return NF_ENOMEM;
+    int v = ctx->cfg.kernel_variant;
+    if (v < 0) {
+        if (box->variant < 0) {
+            nf_status st = autotune(ctx, box, lo, hi);
+            if (st != NF_OK) return st;
         }
-        box->part_bytes = need;
+        v = box->variant;
     }
+    std::unique_ptr<Plan> pl;
+    nf_status st = new_plan(ctx, box, lo, hi, v, pl);
+    if (st != NF_OK) return st;
     *out = pl.get();
     box->plans[key] = std::move(pl);
+    return NF_OK;
+}
+
+extern "C" int nf_kernel_variant_count(void) { return NVARIANTS; }
+
+extern "C" const char *nf_kernel_variant_name(int v) {
+    return (v >= 0 && v < NVARIANTS) ? VARIANTS[v].name : "";
+}
+
+extern "C" nf_status nf_box_tuning(const nf_box *box, int *variant, float *ms, int n) {
+    if (!box || !variant) {
+        set_error("nf_box_tuning: null argument");
+        return NF_EINVAL;
+    }
+    *variant = box->variant;
+    for (int i = 0; ms && i < n && i < NVARIANTS; i++) ms[i] = box->tune_ms[i];
     return NF_OK;
 }
 
@@ -845,5 +990,6 @@ extern "C" nf_status nf_box_forces(nf_ctx *ctx, nf_box *box, int lo, int hi, voi
     ctx->last.padded_pairs = pl->padded_pairs;
     ctx->last.launches = (pl->n_heavy_groups + pl->n_light > 0 ? 1 : 0) + (pl->n_range > 0 ? 1 : 0);
     ctx->last.items = pl->n_heavy_groups * WARPS_PER_CTA + pl->n_light;
+    ctx->last.variant = pl->variant;
     return NF_OK;
 }

@@ -40,7 +40,7 @@ extern "C" void nf_config_default(nf_config *cfg) {
     cfg->accumulation = NF_ACC_COMPENSATED;
     cfg->out_kind = NF_OUT_FLOAT4;
     cfg->sinks_per_lane = 0;
-    cfg->warps_per_cta = 0;
+    cfg->kernel_variant = -1;
 }
 
 static nf_status check_config(const nf_config *c) {
@@ -71,6 +71,10 @@ static nf_status check_config(const nf_config *c) {
     if (c->sinks_per_lane != 0 && c->sinks_per_lane != 1 && c->sinks_per_lane != 2 &&
         c->sinks_per_lane != 4) {
         set_error("sinks_per_lane must be 0, 1, 2 or 4");
+        return NF_EINVAL;
+    }
+    if (c->kernel_variant < -1 || c->kernel_variant >= nf_kernel_variant_count()) {
+        set_error("kernel_variant out of range");
         return NF_EINVAL;
     }
     if (c->out_kind == NF_OUT_FLOAT3 && c->b2 > 0.f) {
@@ -198,7 +202,7 @@ extern "C" nf_status nf_measure_fp32_peak(nf_ctx *ctx, double seconds_sustained,
     }
     std::lock_guard<std::mutex> lk(ctx->mu);
     NF_CUDA(cudaSetDevice(ctx->device));
-    const int threads = 256, blocks = ctx->sms * 8, iters = 2048;
+    const int threads = 256, blocks = ctx->sms * 8, iters = 16384;
     float *out = nullptr;
     NF_CUDA(cudaMalloc(&out, (size_t)blocks * threads * sizeof(float)));
     const double flops = 2.0 * 64.0 * iters * (double)blocks * threads;

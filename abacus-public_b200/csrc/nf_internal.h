@@ -40,6 +40,7 @@ struct Item {
 
 struct Plan {
     int lo = 0, hi = 0;
+    int variant = 0;  // kernel shape (index into the variant table)
     int64_t p0 = 0, n_range = 0;
     Item *d_heavy = nullptr;
     int n_heavy_groups = 0;
@@ -53,6 +54,35 @@ struct Plan {
     cudaGraphExec_t graph = nullptr;
 };
 
+// The pencil engine, shared by the batched form (nf_box.cu) and the plain
+// drop-in (nf_sic.cu).  A launch covers the pencils listed in `items` of a
+// box described by float4 positions and a cell prefix array whose linear
+// cell id is ((x*cpd)+y)*cpd+z for x in [0, nx).
+struct EngineLaunch {
+    const float4 *pos = nullptr;
+    const int64_t *cs = nullptr;
+    int cpd = 0;
+    const Item *heavy = nullptr;  // CTA-split groups (WARPS_PER_CTA items each)
+    int n_heavy_groups = 0;
+    const Item *light = nullptr;
+    int n_light = 0;
+    int *counters = nullptr;      // 2 ints, zeroed by engine_launch
+    double *part = nullptr;       // (2R+1) * nc * n_range doubles
+    int64_t p0 = 0, n_range = 0;  // the sinks' particle range
+    int variant = 0;
+    int grid = 0;                 // CTAs (0: one full wave)
+};
+nf_status engine_launch(nf_ctx *ctx, const EngineLaunch &L, double box_h, cudaStream_t st);
+nf_status engine_coadd(nf_ctx *ctx, const double *part, int64_t n, void *out, cudaStream_t st);
+nf_status engine_pack(nf_ctx *ctx, const float *x, const float *y, const float *z, int64_t n,
+                      float4 *out, cudaStream_t st);
+int engine_grid(nf_ctx *ctx, int variant);
+int engine_variant_smax(int variant);
+int engine_plain_variant();
+constexpr int ENGINE_WARPS_PER_CTA = 8;
+// SIC size limits from a buffer budget (the reference's bytes-per-block model).
+nf_status sic_limits(int out_kind, int cpd, uint64_t max_buffer_bytes, nf_gpu_limits *lim);
+
 }  // namespace nf
 
 struct nf_box {
@@ -65,6 +95,8 @@ struct nf_box {
     float *d_stage = nullptr;         // position upload staging, 3 * np floats
     size_t part_bytes = 0;
     std::map<std::pair<int, int>, std::unique_ptr<nf::Plan>> plans;
+    int variant = -1;       // kernel shape chosen by the autotuner (-1: not tuned yet)
+    float tune_ms[8] = {};  // kernel time of each candidate during tuning
     size_t device_bytes() const;
 };
 

@@ -8,11 +8,11 @@
 //     Newton-Raphson step; for the far field the step is applied to the cube:
 //       y = rsqrt(r2); e = r2*y^2 - 1; r2^-3/2 ~= y^3 * (1 - 1.5 e)
 //     (first-order Newton correction of y, cubed: 5 FP32 instructions).
-//   * the single spline's far branch is accumulated without the 1/eps^2
-//     scaling (g = r^-3, the result is multiplied by eps^3 once per sink);
-//     pairs closer than the softening length take the reference formula,
-//     min(f^3, (-15 f + 6) dr2 + 10) (the fminf form of DirectCPUKernels.cc:71),
-//     times eps^-3.
+//   * the single spline is accumulated in far units, g = f_ref / eps^3
+//     (r^-3 in the far branch), and the sum is multiplied by eps^3 once per
+//     sink.  Source cells that cannot hold a pair closer than one cell width
+//     use the far branch alone; cells adjacent to the sink's cell evaluate
+//     both branches (spline_g_both).
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -56,15 +56,18 @@ __device__ __forceinline__ void two_sum(float a, float b, float &s, float &err) 
 // Kernel constants shared by every pair of a launch.
 struct PairConst {
     float eps;        // the reference kernel parameter (eps^2, 1/eps^2, 1/eps, eps^3)
-    float near_thr;   // single spline: r^2 below which the exact formula is used
+    float near_thr;   // single spline: eps^2 (unscaled)
     float inv_eps3;   // single spline: eps^-3
     float b2;         // FOF density radius^2 (0 = off)
+    // single spline near branch in far units (g = f_ref / eps^3):
+    //   (-15 u + 6 u^2 + 10) / eps^3 with u = r/eps = r^2 y / eps
+    //   = (c1 y + c2) r^2 + c3,  c1 = -15 eps^-4, c2 = 6 eps^-5, c3 = 10 eps^-3
+    float c1, c2, c3;
 };
 
-// Far-field / default evaluation: returns g with a -= g * d.
+// Default evaluation: returns g with a -= g * d.
 // Plummer: (r^2 + eps^2)^-3/2.  Single spline far branch: r^-3 (r^2 floored
-// at 1e-25 so that a self pair stays finite; it is always re-evaluated by
-// the exact path because its r^2 is below near_thr).
+// at 1e-25, far below any eps^2, so that a zero separation stays finite).
 template <int SOFT>
 __device__ __forceinline__ float pair_g_fast(float dx, float dy, float dz, const PairConst &pc,
                                              float &r2_out) {
@@ -104,15 +107,26 @@ __device__ __forceinline__ float pair_g_fast(float dx, float dy, float dz, const
     }
 }
 
-// Single spline, exact reference formula in far units (g * eps^3 = f_ref).
-__device__ __forceinline__ float spline_g_exact(float dx, float dy, float dz,
-                                                const PairConst &pc) {
-    float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-    float dr2 = fmaf(r2, pc.eps, 1e-32f);
-    float f = rsqrt_nr(dr2);
-    float f3 = f * f * f;  // +inf for a self pair; the min picks the polynomial
-    float pn = fmaf(fmaf(-15.0f, f, 6.0f), dr2, 10.0f);
-    return fminf(f3, pn) * pc.inv_eps3;
+// Single spline, both branches, for source cells adjacent to the sink cell
+// (the only ones that can hold pairs closer than eps).  The reference writes
+// it as min(f^3, (-15 f + 6) dr2 + 10) in eps units (DirectCPUKernels.cc:71;
+// the GPU's branch on dr2 > 1, DirectGPUKernels.cuh:94-98, selects the same
+// value because the two branches touch to second order at u = 1 and the
+// polynomial is the smaller one for u < 1).  Here it is evaluated in far
+// units with the Newton-corrected y = 1/r:
+//   g = min(y^3, (c1 y + c2) r^2 + c3)
+// A self pair (d = 0, r^2 = 1e-25 floor) gives a finite g times d = 0; a
+// padding record far away gives an infinite polynomial and g ~ 0.
+__device__ __forceinline__ float spline_g_both(float dx, float dy, float dz,
+                                               const PairConst &pc) {
+    float r2 = fmaf(dz, dz, fmaf(dy, dy, fmaf(dx, dx, 1e-25f)));
+    float y = rsqrt_est(r2);
+    float y2 = y * y;
+    float e = fmaf(r2, y2, -1.0f);
+    float yn = fmaf(-0.5f * e, y, y);
+    float gfar = yn * yn * yn;
+    float gnear = fmaf(fmaf(pc.c1, yn, pc.c2), r2, pc.c3);
+    return fminf(gfar, gnear);
 }
 
 // Unsoftened r^2 for the FOF density sum (w += b2 - r^2 if r^2 < b2).

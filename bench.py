@@ -56,6 +56,11 @@ WORKLOADS = {
                       desc="64^3 uniform particles, cpd 17, Plummer eps=spacing/40"),
     "clustered512": dict(n_side=512, cpd=125, softening=1, kind="clustered", seed=3,
                          desc="512^3 particles, cpd 125, clustered mixture as clustered256"),
+    "clustered128": dict(n_side=128, cpd=33, softening=1, kind="clustered", seed=4,
+                         desc="128^3 particles, cpd 33, clustered mixture as clustered256 "
+                              "(the profiling case)"),
+    "uniform256": dict(n_side=256, cpd=65, softening=0, kind="uniform", seed=5,
+                       desc="256^3 uniform particles, cpd 65, Plummer eps=spacing/40"),
 }
 
 
@@ -299,7 +304,7 @@ def our_arm(args, w):
     stream = torch.cuda.Stream(device=local)
     torch.cuda.set_stream(stream)
     ctx.set_stream(stream.cuda_stream)  # the library launches on the stream the events time
-    peak_burst, peak_sust = ctx.fp32_peak(1.0)
+    peak_burst, peak_sust = (float("nan"), float("nan")) if args.profile else ctx.fp32_peak(1.0)
     db = ctx.box(box)
     pairs = db.pair_count()
     n = box.n
@@ -331,6 +336,15 @@ def our_arm(args, w):
     value = total_pairs / (ms_per_step / 1e3)
     launches = args.steps * t.launches
 
+    if args.profile:
+        t = ctx.last_timing()
+        if rank == 0:
+            print(json.dumps({"profile_run": args.workload, "ms_per_step": ms_per_step,
+                              "kernel_ms": float(np.mean(kernel_ms)), "pairs": pairs,
+                              "pairs_per_s": value}), flush=True)
+        db.close()
+        ctx.close()
+        return 0
     # end to end through the C ABI with pinned host buffers: H2D positions,
     # sweep, D2H accelerations, every step
     hx = torch.from_numpy(box.x).pin_memory()
@@ -364,6 +378,11 @@ def our_arm(args, w):
             db.forces_device(s, s + 1, out_dev.data_ptr())
             lat.append(1e3 * (time.perf_counter() - t0))
 
+    tv, tms = db.tuning()
+    lib = capi.lib()
+    tune_info = {"variant": tv, "shape": lib.nf_kernel_variant_name(tv).decode(),
+                 "candidates_ms": {lib.nf_kernel_variant_name(i).decode(): round(m, 3)
+                                   for i, m in enumerate(tms) if m > 0}}
     flops = FLOPS_PER_PAIR[soft]
     k_ms = float(np.mean(kernel_ms))
     achieved = pairs * flops / (k_ms / 1e3) / 1e12
@@ -399,6 +418,7 @@ def our_arm(args, w):
                 "h2d_bytes_per_step": int(12 * n), "d2h_bytes_per_step": int(16 * n)},
         "gpu_launches": int(launches),
         "clocks": clocks,
+        "autotune": tune_info,
     }
     if rank == 0 and not args.no_cpu_baseline:
         rate, threads, desc, kind, _, _ = cpu_reference_rate(box, w, target_s=args.cpu_seconds)
@@ -407,7 +427,7 @@ def our_arm(args, w):
         # precision of this run's result against the FP64 oracle (checker)
         sys.path.insert(0, str(ROOT / "oracle"))
         import oracle
-        a = out_dev.cpu().numpy()
+        a = oa  # the last full sweep, returned to the caller's host buffer
         sinks = np.sort(np.random.default_rng(5).choice(n, 2000, replace=False))
         rms, mx, _ = oracle.frac_errors(a[sinks, :3], oracle.fp64_sinks(box, soft, eps, sinks))
         result["accuracy_vs_fp64"] = {"rms_frac": rms, "max_frac": mx, "sinks": 2000}
@@ -430,6 +450,9 @@ def main():
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="clustered256")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--profile", action="store_true",
+                    help="timed sweeps only (no peak probe, CPU baseline, e2e or latency "
+                         "phases): the command profiled under ncu")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

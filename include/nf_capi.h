@@ -86,14 +86,16 @@ typedef struct nf_config {
     float b2;               /* FOF density radius^2 (WriteState.DensityKernelRad2); 0 = off */
     int accumulation;       /* NF_ACC_* */
     int out_kind;           /* NF_OUT_* */
-    int sinks_per_lane;     /* 0 = autotuned tile shapes; else force 1, 2 or 4 */
-    int warps_per_cta;      /* 0 = autotuned; else 4 or 8 */
+    int sinks_per_lane;     /* 0 = tile shapes from the occupancy; else cap at 1, 2 or 4 */
+    int kernel_variant;     /* -1 = autotuned per box; else a fixed kernel shape
+                               0 .. nf_kernel_variant_count()-1 */
 } nf_config;
 
 typedef struct nf_ctx nf_ctx;
 typedef struct nf_box nf_box;
 
-/* Fill *cfg with defaults (device 0, R 2, single spline, compensated, float4). */
+/* Fill *cfg with defaults (device 0, R 2, single spline, compensated, float4,
+ * autotuned kernel shape). */
 void nf_config_default(nf_config *cfg);
 
 nf_status nf_init(const nf_config *cfg, nf_ctx **out);
@@ -180,6 +182,103 @@ nf_status nf_sic_execute(nf_ctx *ctx, const nf_sic_desc *sic, int jlow, int jhig
 /* Wait for every queued SIC (bounded). */
 nf_status nf_sic_drain(nf_ctx *ctx, uint64_t timeout_ns);
 
+/* ---------------- 2b. NearFieldDriver and the SIC planner ---------------- */
+/* The host side of the drop-in: a C++ NearFieldDriver with the reference's
+ * methods (singlestep/Timestep/directdriver.cpp:22-95) and a
+ * SetInteractionCollection planner (PencilOnPencil.cc:180-418), driven
+ * through these entry points.  The abacus globals they read (CP, SB, SS, P)
+ * are replaced by per-slab views registered by the caller. */
+
+/* cellinfo, singlestep/DataModel/particlestruct.cpp:334-346 (same layout). */
+typedef struct nf_cellinfo {
+    uint64_t startindex;
+    uint64_t startindex_with_ghost;
+    int32_t count;
+    int32_t active;
+    float mean_square_velocity;
+    float max_component_velocity;
+    float max_component_acceleration;
+} nf_cellinfo;
+
+/* One x-slab as abacus holds it. */
+typedef struct nf_slab_view {
+    const float *posxyz;          /* PosXYZSlab: X[nslab] | Y[nslab] | Z[nslab] */
+    uint64_t nslab;               /* SS->size_with_ghost(slab) */
+    const nf_cellinfo *cellinfo;  /* CellInfoSlab: cpd*cpd cells, (y, z) order */
+    void *acc;                    /* AccSlab: one accstruct per particle (sink slabs) */
+} nf_slab_view;
+
+typedef struct nf_driver_params {
+    int device;
+    int cpd;
+    int64_t np;
+    int near_field_radius;         /* P.NearFieldRadius */
+    int softening;                 /* NF_SOFT_* (configure --with-softening) */
+    double softening_length;       /* ReadState.SofteningLengthNow / BoxSize (Plummer-equivalent) */
+    float density_kernel_rad2;     /* WriteState.DensityKernelRad2 (b2; 0 = no density) */
+    int direct_bpd;                /* P.DirectBPD */
+    double mem_per_gpu_buffer_gb;  /* P.MemPerGPUBufferGB (0 = auto) */
+    double max_ram_mb;             /* P.MAXRAMMB (auto buffer sizing) */
+    int use_pinned_gpu_memory;     /* P.UsePinnedGPUMemory (-1 = auto) */
+    int accumulation;              /* NF_ACC_* */
+    int out_kind;                  /* NF_OUT_* (accstruct) */
+} nf_driver_params;
+
+/* NearFieldDriver statistics (directdriver.cpp:41-77, filled by Finalize and
+ * AggregateStats, directdriver.cpp:434-526). */
+typedef struct nf_driver_stats {
+    uint64_t direct_interactions;         /* TotalDirectInteractions_GPU */
+    uint64_t padded_direct_interactions;  /* TotalPaddedDirectInteractions_GPU */
+    double gdi_gpu, gdi_padded_gpu;       /* the above / 1e9 */
+    double total_gb_to, total_gb_from;
+    double total_sinks, total_sources, total_padded_sinks, total_padded_sources;
+    double mean_splits_per_slab;
+    int max_nsplits;
+    double gpu_throughput_time;           /* s with at least one SIC in flight */
+    double calc_split_s, sic_construction_s, sic_execute_s, finalize_s;
+    double softening_length_internal;
+    float eps;
+    int ngpu, nbuffers;
+    int max_sink_blocks, max_source_blocks;
+} nf_driver_stats;
+
+typedef struct nf_driver nf_driver;
+
+/* NearFieldDriver::NearFieldDriver(int NearFieldRadius) (directdriver.cpp:105-203):
+ * eps per softening, GPU count, buffer sizing, GPUSetup. */
+nf_status nf_driver_create(const nf_driver_params *p, nf_driver **out);
+/* Register slab `slab`'s data (positions, cellinfo, acceleration arena).
+ * Slabs slab-R .. slab+R must be registered before ExecuteSlab(slab). */
+nf_status nf_driver_set_slab(nf_driver *drv, int slab, const nf_slab_view *view);
+/* ExecuteSlab / ExecuteSlabGPU (directdriver.cpp:242-409): split the slab
+ * into y-ranges fitting the GPU buffers, build the SICs, queue them. */
+nf_status nf_driver_execute_slab(nf_driver *drv, int slab, int blocking);
+/* SlabDone (directdriver.cpp:414-431): 1 when every SIC of the slab has
+ * completed, 0 while in flight, -1 if one failed. */
+int nf_driver_slab_done(nf_driver *drv, int slab);
+/* Finalize (directdriver.cpp:434-492): collect SIC statistics, free them. */
+nf_status nf_driver_finalize(nf_driver *drv, int slab);
+/* AggregateStats (directdriver.cpp:498-526). */
+nf_status nf_driver_aggregate_stats(nf_driver *drv, nf_driver_stats *stats);
+/* The underlying context (to share with nf_box_* calls). */
+nf_ctx *nf_driver_context(nf_driver *drv);
+void nf_driver_destroy(nf_driver *drv);
+
+/* The SetInteractionCollection planner alone (no GPU): plan rows
+ * [jlow, jhigh) of slab `slab` over registered slabs and return its sizes
+ * and counters (NSinkSets, NSourceSets, NSinkBlocks, NSourceBlocks,
+ * InteractionCount, DirectTotal, PaddedDirectTotal, SinkTotal, SourceTotal).
+ * Arrays, when non-NULL, receive SinkSetCount[nsinksets],
+ * SinkBlockParentPencil[nsinkblocks], SourceSetCount[nsourcesets]. */
+typedef struct nf_sic_summary {
+    int nsinksets, nsourcesets, nsinkblocks, nsourceblocks, interaction_count;
+    uint64_t direct_total, padded_direct_total, sink_total, source_total;
+    uint64_t padded_sink_total, padded_source_total;
+} nf_sic_summary;
+nf_status nf_driver_plan_sic(nf_driver *drv, int slab, int jlow, int jhigh, nf_sic_summary *sum,
+                             int32_t *sink_set_count, int32_t *sink_block_parent,
+                             int32_t *source_set_count);
+
 /* ---------------- 3. batched form: a box resident in HBM ---------------- */
 /* Upload a box: cpd^3 cells, particles sorted by cell id ((cx*cpd)+cy)*cpd+cz,
  * float32 positions relative to the cell centre given as three host arrays,
@@ -215,9 +314,19 @@ typedef struct nf_timing {
     uint64_t padded_pairs;/* pairs including null-padded lanes/sources */
     int launches;         /* kernel launches of the call */
     int items;            /* warp work items */
+    int variant;          /* kernel shape that ran */
 } nf_timing;
 /* Timing of the last nf_box_forces on this context. */
 nf_status nf_last_timing(nf_ctx *ctx, nf_timing *t);
+
+/* Kernel shapes the autotuner chooses among (sinks per lane, unroll depth,
+ * CTAs per SM).  The first nf_box_forces call on a box times every shape on
+ * the requested slab range and keeps the fastest for that box. */
+int nf_kernel_variant_count(void);
+const char *nf_kernel_variant_name(int variant);
+/* The box's chosen shape (-1 before tuning) and the kernel time of each
+ * candidate during tuning (ms[0 .. n-1]). */
+nf_status nf_box_tuning(const nf_box *box, int *variant, float *ms, int n);
 
 /* Run the context's work on the caller's CUDA stream (a cudaStream_t passed
  * as void*); NULL restores the library's own non-blocking stream. */

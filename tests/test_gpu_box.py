@@ -153,15 +153,33 @@ def test_radius_one_and_float3(capi, oracle, synth):
     assert rms <= FP64_RMS, rms
 
 
-def test_forced_tile_shapes_agree(capi, synth):
+@pytest.mark.parametrize("soft", [0, 1])
+def test_kernel_shapes_agree(capi, synth, soft):
+    """Every kernel shape the autotuner can pick, and forced tile sizes, give
+    the same accelerations to rounding; the autotuner records its timings."""
     box = synth.clustered_box(30000, 11, seed=11, n_clumps=25)
-    eps = synth.kernel_eps(1, synth.plummer_eps(31))
+    eps = synth.kernel_eps(soft, synth.plummer_eps(31))
     outs = []
-    for S in (1, 2, 4, 0):
-        with capi.Context(softening=1, eps=eps, sinks_per_lane=S) as ctx:
+    nv = capi.lib().nf_kernel_variant_count()
+    assert nv >= 4
+    for v in range(nv):
+        with capi.Context(softening=soft, eps=eps, kernel_variant=v) as ctx:
+            db = ctx.box(box)
+            outs.append(db.forces())
+            assert ctx.last_timing().variant == v
+            db.close()
+    for S in (1, 2):
+        with capi.Context(softening=soft, eps=eps, sinks_per_lane=S) as ctx:
             db = ctx.box(box)
             outs.append(db.forces())
             db.close()
+    with capi.Context(softening=soft, eps=eps) as ctx:
+        db = ctx.box(box)
+        outs.append(db.forces())
+        v, ms = db.tuning()
+        assert 0 <= v < nv and ctx.last_timing().variant == v
+        assert all(m > 0 for m in ms) and ms[v] == min(ms)
+        db.close()
     for o in outs[1:]:
         np.testing.assert_allclose(o, outs[0], rtol=0, atol=2e-6 * np.abs(outs[0]).max())
 
