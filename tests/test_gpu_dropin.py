@@ -47,7 +47,7 @@ def test_driver_small_buffers_split_more(capi, oracle, synth):
     box = synth.uniform_box(80000, 15, seed=42)
     length = synth.plummer_eps(43)
     outs, splits = [], []
-    for mem in (0.0, 0.004):
+    for mem in (0.0, 0.0012):  # 1.2 MB: ~190 sink blocks per SIC
         drv = capi.Driver(box, softening=0, softening_length=length, direct_bpd=2, mem_gb=mem)
         try:
             outs.append(drv.run_all())
