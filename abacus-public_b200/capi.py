@@ -159,6 +159,9 @@ EXPORTS = {
                                          ctypes.c_int, ctypes.POINTER(ctypes.c_uint64)]),
     "nf_last_timing": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Timing)]),
     "nf_set_stream": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "nf_forces_noalloc": (ctypes.c_int, [ctypes.POINTER(Config), ctypes.c_int, ctypes.c_void_p,
+                                         ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                         ctypes.c_void_p, ctypes.c_void_p]),
     "nf_kernel_variant_count": (ctypes.c_int, []),
     "nf_kernel_variant_name": (ctypes.c_char_p, [ctypes.c_int]),
     "nf_box_tuning": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),

@@ -993,3 +993,150 @@ extern "C" nf_status nf_box_forces(nf_ctx *ctx, nf_box *box, int lo, int hi, voi
     ctx->last.variant = pl->variant;
     return NF_OK;
 }
+
+// ------------------------------------------------------------------------
+// Allocation-free entry point (nf_forces_noalloc)
+//
+// For callers that cannot allocate device memory: code running where
+// cudaMalloc is off limits (inside another framework's memory pool, a
+// caching allocator that owns the device, or a context whose allocations
+// are frozen after start-up).  The caller passes device inputs and outputs;
+// the only scratch is the file-scope array below, which every GPU that loads
+// this library holds until the process exits.
+// ------------------------------------------------------------------------
+namespace nf {
+
+constexpr int64_t NOALLOC_MAX_SINKS = 196608;             // particles per call
+constexpr size_t NOALLOC_SCRATCH_BYTES = (size_t)32 << 20;  // 32 MiB
+constexpr size_t NOALLOC_COUNTER_BYTES = 256;
+static_assert(NOALLOC_COUNTER_BYTES + (size_t)MAXW * 4 * 8 * NOALLOC_MAX_SINKS <= NOALLOC_SCRATCH_BYTES,
+              "scratch holds (2R+1) x 4 double partials per sink");
+// [0, 256): work counters; then (2R+1) x nc x n doubles of pencil partials.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
+
+// Warps take whole pencils from a counter and run their tiles in order.
+template <int SOFT, bool DENS>
+__global__ void __launch_bounds__(WARPS_PER_CTA * 32, 2)
+    noalloc_pencil_kernel(KParams kp, int pencil0, int n_pencils) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    WarpSmem &ws = reinterpret_cast<WarpSmem *>(smem_raw)[threadIdx.x >> 5];
+    const int lane = threadIdx.x & 31;
+    const int W = 2 * kp.R + 1;
+    for (;;) {
+        int q = 0;
+        if (lane == 0) q = atomicAdd(&kp.counters[1], 1);
+        q = __shfl_sync(FULL, q, 0);
+        if (q >= n_pencils) break;
+        Item it{pencil0 + q, 0, 0, 4, 0, 0, 0, 0};
+        setup_tables(kp, it, ws, lane);
+        const int np_ = ws.spre[W];
+        it.src_end = ws.cpre[W * W];
+        for (int b = 0; b < np_; b += TILE_MAX) {
+            it.sink_begin = b;
+            it.nsink = min(TILE_MAX, np_ - b);
+            if (it.nsink <= 32)
+                run_tile<SOFT, DENS, 1, 8>(kp, ws, it, lane, nullptr, 0);
+            else if (it.nsink <= 64)
+                run_tile<SOFT, DENS, 2, 8>(kp, ws, it, lane, nullptr, 0);
+            else
+                run_tile<SOFT, DENS, 4, 8>(kp, ws, it, lane, nullptr, 0);
+        }
+    }
+}
+
+typedef void (*NoallocFn)(KParams, int, int);
+
+static NoallocFn noalloc_kernel(int soft, bool dens) {
+    switch (soft) {
+    case SOFT_PLUMMER: return dens ? noalloc_pencil_kernel<SOFT_PLUMMER, true> : noalloc_pencil_kernel<SOFT_PLUMMER, false>;
+    case SOFT_SINGLE_SPLINE:
+        return dens ? noalloc_pencil_kernel<SOFT_SINGLE_SPLINE, true> : noalloc_pencil_kernel<SOFT_SINGLE_SPLINE, false>;
+    case SOFT_CUBIC_SPLINE:
+        return dens ? noalloc_pencil_kernel<SOFT_CUBIC_SPLINE, true> : noalloc_pencil_kernel<SOFT_CUBIC_SPLINE, false>;
+    default:
+        return dens ? noalloc_pencil_kernel<SOFT_CUBIC_PLUMMER, true> : noalloc_pencil_kernel<SOFT_CUBIC_PLUMMER, false>;
+    }
+}
+
+static std::mutex g_noalloc_mu;
+static void *g_noalloc_base[128];  // device address of the scratch, per device ordinal
+
+}  // namespace nf
+
+extern "C" nf_status nf_forces_noalloc(const nf_config *cfg, int cpd, const void *pos,
+                                       const int64_t *cell_start, int slab_lo, int slab_hi,
+                                       void *out, void *stream) {
+    if (!cfg || !pos || !cell_start || !out) {
+        set_error("nf_forces_noalloc: null argument");
+        return NF_EINVAL;
+    }
+    const int R = cfg->near_field_radius;
+    if (R < 1 || R > 2 || cpd < 2 * R + 1 || (cpd & 1) == 0 || slab_lo < 0 || slab_hi > cpd ||
+        slab_lo >= slab_hi || cfg->softening < 0 || cfg->softening > 3 ||
+        !std::isfinite(cfg->eps) || cfg->eps <= 0.f || !(cfg->b2 >= 0.f) ||
+        (cfg->out_kind != NF_OUT_FLOAT3 && cfg->out_kind != NF_OUT_FLOAT4) ||
+        (cfg->out_kind == NF_OUT_FLOAT3 && cfg->b2 > 0.f)) {
+        set_error("nf_forces_noalloc: bad configuration or slab range");
+        return NF_EINVAL;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    int dev = 0;
+    NF_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 128) {
+        set_error("nf_forces_noalloc: device ordinal beyond 127");
+        return NF_EINVAL;
+    }
+    void *base = nullptr;
+    {
+        // once per device, with that device current: the array's device address
+        std::lock_guard<std::mutex> lk(g_noalloc_mu);
+        if (!g_noalloc_base[dev]) {
+            void *p = nullptr;
+            cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+            if (e != cudaSuccess) return cuda_fail(e, "nf_forces_noalloc: cudaGetSymbolAddress");
+            g_noalloc_base[dev] = p;
+        }
+        base = g_noalloc_base[dev];
+    }
+    const int64_t c2 = (int64_t)cpd * cpd;
+    int64_t bounds[2] = {0, 0};
+    NF_CUDA(cudaMemcpyAsync(&bounds[0], cell_start + slab_lo * c2, sizeof(int64_t),
+                            cudaMemcpyDeviceToHost, st));
+    NF_CUDA(cudaMemcpyAsync(&bounds[1], cell_start + slab_hi * c2, sizeof(int64_t),
+                            cudaMemcpyDeviceToHost, st));
+    NF_CUDA(cudaStreamSynchronize(st));
+    const int64_t n = bounds[1] - bounds[0];
+    if (n < 0 || n > NOALLOC_MAX_SINKS) {
+        set_error("nf_forces_noalloc: at most 196608 particles in the requested slabs "
+                  "(32 MiB static scratch)");
+        return NF_EINVAL;
+    }
+    if (n == 0) return NF_OK;
+    nf_ctx tmp;  // parameters only; no stream, event or memory of its own
+    tmp.cfg = *cfg;
+    tmp.device = dev;
+    NF_CUDA(cudaDeviceGetAttribute(&tmp.sms, cudaDevAttrMultiProcessorCount, dev));
+    NF_CUDA(cudaMemsetAsync(base, 0, NOALLOC_COUNTER_BYTES, st));
+    EngineLaunch L;
+    L.pos = (const float4 *)pos;
+    L.cs = cell_start;
+    L.cpd = cpd;
+    L.counters = (int *)base;
+    L.part = (double *)((char *)base + NOALLOC_COUNTER_BYTES);
+    L.p0 = bounds[0];
+    L.n_range = n;
+    KParams kp = params_from(&tmp, L);
+    NoallocFn fn = noalloc_kernel(cfg->softening, cfg->b2 > 0.f);
+    const size_t smem = sizeof(WarpSmem) * WARPS_PER_CTA;
+    int per_sm = 1;
+    NF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)fn,
+                                                          WARPS_PER_CTA * 32, smem));
+    int pencil0 = (int)(slab_lo * c2), npen = (int)((slab_hi - slab_lo) * c2);
+    void *args[] = {&kp, &pencil0, &npen};
+    NF_CUDA(cudaLaunchKernel((const void *)fn, dim3(tmp.sms * std::max(per_sm, 1)),
+                             dim3(WARPS_PER_CTA * 32), args, smem, st));
+    coadd_kernel<<<tmp.sms * 8, 256, 0, st>>>(L.part, n, 2 * R + 1, kp.nc, output_scale(*cfg),
+                                              cfg->out_kind, out);
+    NF_CUDA(cudaGetLastError());
+    return NF_OK;
+}

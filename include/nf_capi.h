@@ -328,6 +328,28 @@ const char *nf_kernel_variant_name(int variant);
  * candidate during tuning (ms[0 .. n-1]). */
 nf_status nf_box_tuning(const nf_box *box, int *variant, float *ms, int n);
 
+/* Allocation-free variant of the batched sweep (no counterpart in the
+ * reference).  For callers that cannot call cudaMalloc -- code that runs
+ * inside another framework's memory pool or caching allocator, or in a
+ * process whose device allocations are fixed after start-up.  Nothing is
+ * allocated on the device or the host: the scratch (pencil partials and a
+ * work counter) is one 32 MiB static device array, held by every GPU that
+ * loads this library until the process exits.
+ *   pos        device float4 records (x, y, z, unused) in cell order
+ *   cell_start device int64 prefix offsets, cpd^3 + 1 entries
+ *   out        device records (cfg->out_kind) for the particles of slabs
+ *              [slab_lo, slab_hi), in particle order
+ *   stream     a cudaStream_t, or NULL for the default stream
+ * At most 196608 particles in the requested slabs; more is NF_EINVAL.  The
+ * first call on each device looks up the array's device address with that
+ * device current; make that first call before any stream capture.  All
+ * calls share the one array and it keeps the last call's contents: calls
+ * that overlap on the GPU (other streams, other host threads) race.  The
+ * call returns once the work is queued on `stream`. */
+nf_status nf_forces_noalloc(const nf_config *cfg, int cpd, const void *pos,
+                            const int64_t *cell_start, int slab_lo, int slab_hi, void *out,
+                            void *stream);
+
 /* Run the context's work on the caller's CUDA stream (a cudaStream_t passed
  * as void*); NULL restores the library's own non-blocking stream. */
 nf_status nf_set_stream(nf_ctx *ctx, void *stream);
