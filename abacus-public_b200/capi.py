@@ -117,8 +117,37 @@ class SicSummary(ctypes.Structure):
                 ("padded_source_total", ctypes.c_uint64)]
 
 
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("hbm_budget_bytes", ctypes.c_size_t), ("max_inflight", ctypes.c_int),
+                ("max_queued", ctypes.c_int)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_uint64), ("admitted", ctypes.c_uint64),
+                ("completed", ctypes.c_uint64), ("failed", ctypes.c_uint64),
+                ("rejected", ctypes.c_uint64), ("cancelled", ctypes.c_uint64),
+                ("pairs", ctypes.c_uint64), ("busy_s", ctypes.c_double),
+                ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double),
+                ("mean_ms", ctypes.c_double), ("max_ms", ctypes.c_double),
+                ("queue_p50_ms", ctypes.c_double), ("queue_p99_ms", ctypes.c_double),
+                ("max_concurrent", ctypes.c_int), ("hbm_budget_bytes", ctypes.c_size_t),
+                ("hbm_peak_bytes", ctypes.c_size_t)]
+
+
 # Every symbol the header declares; the loader checks each one is exported.
 EXPORTS = {
+    "nf_server_start": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ServerConfig),
+                                       ctypes.POINTER(ctypes.c_void_p)]),
+    "nf_server_submit": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                        ctypes.c_void_p, ctypes.c_int,
+                                        ctypes.POINTER(ctypes.c_uint64)]),
+    "nf_server_poll": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64,
+                                      ctypes.POINTER(ctypes.c_int)]),
+    "nf_server_wait": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64]),
+    "nf_server_cancel": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64]),
+    "nf_server_stats_get": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ServerStats)]),
+    "nf_server_stats_reset": (ctypes.c_int, [ctypes.c_void_p]),
+    "nf_server_stop": (None, [ctypes.c_void_p]),
     "nf_driver_create": (ctypes.c_int, [ctypes.POINTER(DriverParams),
                                         ctypes.POINTER(ctypes.c_void_p)]),
     "nf_driver_set_slab": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int,
@@ -437,3 +466,53 @@ class Driver:
                     raise NfError(NF_ETIMEDOUT, "slabs still in flight")
                 time.sleep(0.001)
         return self.slabs.gather_acc(self.box.n)
+
+
+class Server:
+    """nf_server: slab requests over resident boxes, continuous admission."""
+
+    def __init__(self, ctx: Context, hbm_budget_bytes: int = 0, max_inflight: int = 8,
+                 max_queued: int = 65536):
+        self.ctx = ctx
+        cfg = ServerConfig(hbm_budget_bytes, max_inflight, max_queued)
+        h = ctypes.c_void_p()
+        check(lib().nf_server_start(ctx.h, ctypes.byref(cfg), ctypes.byref(h)), "nf_server_start")
+        self.h = h
+
+    def submit(self, box: DeviceBox, slab: int, out, out_on_device: bool = False) -> int:
+        """Queue slab `slab` of `box`; `out` is a host numpy array or a device pointer."""
+        t = ctypes.c_uint64()
+        ptr = out if out_on_device else out.ctypes.data
+        check(lib().nf_server_submit(self.h, box.h, slab, ctypes.c_void_p(ptr),
+                                     int(out_on_device), ctypes.byref(t)), "nf_server_submit")
+        return t.value
+
+    def poll(self, ticket: int) -> int:
+        s = ctypes.c_int()
+        check(lib().nf_server_poll(self.h, ticket, ctypes.byref(s)), "nf_server_poll")
+        return s.value
+
+    def wait(self, ticket: int, timeout_s: float = 120.0):
+        check(lib().nf_server_wait(self.h, ticket, int(timeout_s * 1e9)), "nf_server_wait")
+
+    def cancel(self, ticket: int):
+        check(lib().nf_server_cancel(self.h, ticket), "nf_server_cancel")
+
+    def stats(self) -> ServerStats:
+        s = ServerStats()
+        check(lib().nf_server_stats_get(self.h, ctypes.byref(s)), "nf_server_stats_get")
+        return s
+
+    def reset_stats(self):
+        check(lib().nf_server_stats_reset(self.h), "nf_server_stats_reset")
+
+    def close(self):
+        if self.h:
+            lib().nf_server_stop(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

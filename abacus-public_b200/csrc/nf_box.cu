@@ -61,13 +61,21 @@ struct KParams {
     float xyshift[MAXW];  // n h, n = -R .. R
     signed char odx[MAXSRC], ody[MAXSRC];  // source cell order: outer ring first
     int n_outer;                           // cells with max(|dx|,|dy|) == 2
+    // single spline: a source in a cell adjacent to the pencil's column can
+    // be closer than eps to one of the pencil's sinks only if it lies within
+    // eps of the shared face, i.e. (own-cell frame) x < face_lo for dx = +1,
+    // x > face_hi for dx = -1 (likewise y)
+    float face_lo, face_hi;
 };
 
+constexpr int CHUNK = 64;  // sources staged per chunk (two per lane)
+
 struct WarpSmem {
-    float4 buf[32];
+    float4 buf[CHUNK];
     int64_t cstart[MAXSRC];
     int32_t cpre[MAXSRC + 1];
     float csx[MAXSRC], csy[MAXSRC];
+    float4 cnear[MAXSRC];  // per source cell: x range, y range of near-capable sources
     int64_t sstart[MAXW];
     int32_t spre[MAXW + 1];
 };
@@ -99,6 +107,16 @@ __device__ void setup_tables(const KParams &kp, const Item &it, WarpSmem &ws, in
         ws.cstart[lane] = st;
         ws.csx[lane] = kp.xyshift[dx + R];
         ws.csy[lane] = kp.xyshift[dy + R];
+        // near-capable ranges: everything for dx = 0, the face slab for
+        // |dx| = 1, nothing for |dx| = 2 (empty range)
+        const float INF = 3.0e38f;
+        float xl = -INF, xh = INF, yl = -INF, yh = INF;
+        if (dx == 1) xh = kp.face_lo;
+        if (dx == -1) xl = kp.face_hi;
+        if (dy == 1) yh = kp.face_lo;
+        if (dy == -1) yl = kp.face_hi;
+        if (dx > 1 || dx < -1 || dy > 1 || dy < -1) xl = INF, xh = -INF;
+        ws.cnear[lane] = make_float4(xl, xh, yl, yh);
     }
     int incl = warp_incl_scan(cnt, lane);
     if (lane < nsrc) ws.cpre[lane + 1] = incl;
@@ -116,13 +134,20 @@ __device__ void setup_tables(const KParams &kp, const Item &it, WarpSmem &ws, in
     __syncwarp();
 }
 
-// Source record for stream index i (null record far away past the end).
+// Source record for stream index i (null record far away past the end), in
+// the pencil frame.  FLAG: w = 1 if the source may lie within eps of a sink
+// of the pencil (single spline), else 0.
+template <bool FLAG>
 __device__ __forceinline__ float4 load_src(const KParams &kp, const WarpSmem &ws, int i,
                                            int src_end, int &k) {
     if (i >= src_end) return make_float4(1e18f, 1e18f, 1e18f, 0.f);
     while (i >= ws.cpre[k + 1]) k++;
     int64_t p = ws.cstart[k] + (i - ws.cpre[k]);
     float4 t = __ldg(&kp.pos[p]);
+    if (FLAG) {
+        float4 nr = ws.cnear[k];
+        t.w = (t.x >= nr.x && t.x <= nr.y && t.y >= nr.z && t.y <= nr.w) ? 1.f : 0.f;
+    }
     t.x += ws.csx[k];
     t.y += ws.csy[k];
     return t;
@@ -209,33 +234,39 @@ __device__ void run_tile(const KParams &kp, WarpSmem &ws, const Item &it, int la
 #pragma unroll
     for (int s = 0; s < S; s++)
         hx[s] = hy[s] = hz[s] = lx[s] = ly[s] = lz[s] = px[s] = py[s] = pz[s] = pw[s] = 0.f;
-    const int inner_begin = ws.cpre[kp.n_outer];
+    constexpr bool FLAG = SOFT == SOFT_SINGLE_SPLINE;
     const bool plain = kp.plain;
-    int k = 0;
+    int k0 = 0, k1 = 0;
     int base = it.src_begin;
-    float4 pre = load_src(kp, ws, base + lane, it.src_end, k);
-    int nchunk = 0;
-    for (; base < it.src_end; base += 32) {
+    // two sources per lane per chunk: stream indices base+lane, base+32+lane
+    float4 pre0 = load_src<FLAG>(kp, ws, base + lane, it.src_end, k0);
+    float4 pre1 = load_src<FLAG>(kp, ws, base + 32 + lane, it.src_end, k1);
+    for (; base < it.src_end; base += CHUNK) {
+        // a chunk takes the both-branch path only if one of its sources may
+        // lie within eps of one of the tile's sinks
+        bool near = FLAG && __any_sync(FULL, pre0.w + pre1.w != 0.f);
         __syncwarp();
-        ws.buf[lane] = pre;
+        ws.buf[lane] = pre0;
+        ws.buf[lane + 32] = pre1;
         __syncwarp();
-        if (base + 32 < it.src_end) pre = load_src(kp, ws, base + 32 + lane, it.src_end, k);
-        int m = min(32, it.src_end - base);
-        int m_pad = (m + UNR - 1) / UNR * UNR;
-        if (SOFT == SOFT_SINGLE_SPLINE && base + 32 > inner_begin)
-            chunk_pairs<SOFT, DENS, S, true, UNR>(ws.buf, m_pad, sx, sy, sz, px, py, pz, pw, kp.pc);
-        else
-            chunk_pairs<SOFT, DENS, S, false, UNR>(ws.buf, m_pad, sx, sy, sz, px, py, pz, pw, kp.pc);
-        if (++nchunk == 2) {  // fold every 64 sources
-            nchunk = 0;
-            fold<S>(hx, lx, px, plain);
-            fold<S>(hy, ly, py, plain);
-            fold<S>(hz, lz, pz, plain);
+        if (base + CHUNK < it.src_end) {
+            pre0 = load_src<FLAG>(kp, ws, base + CHUNK + lane, it.src_end, k0);
+            pre1 = load_src<FLAG>(kp, ws, base + CHUNK + 32 + lane, it.src_end, k1);
         }
+        int m = min(CHUNK, it.src_end - base);
+        int m_pad = (m + UNR - 1) / UNR * UNR;
+        if constexpr (FLAG) {
+            if (near)
+                chunk_pairs<SOFT, DENS, S, true, UNR>(ws.buf, m_pad, sx, sy, sz, px, py, pz, pw, kp.pc);
+            else
+                chunk_pairs<SOFT, DENS, S, false, UNR>(ws.buf, m_pad, sx, sy, sz, px, py, pz, pw, kp.pc);
+        } else {
+            chunk_pairs<SOFT, DENS, S, false, UNR>(ws.buf, m_pad, sx, sy, sz, px, py, pz, pw, kp.pc);
+        }
+        fold<S>(hx, lx, px, plain);  // fold every 64 sources
+        fold<S>(hy, ly, py, plain);
+        fold<S>(hz, lz, pz, plain);
     }
-    fold<S>(hx, lx, px, plain);
-    fold<S>(hy, ly, py, plain);
-    fold<S>(hz, lz, pz, plain);
 #pragma unroll
     for (int s = 0; s < S; s++) {
         int j = s * 32 + lane;
@@ -243,7 +274,8 @@ __device__ void run_tile(const KParams &kp, WarpSmem &ws, const Item &it, int la
         double vx = (double)hx[s] + (double)lx[s];
         double vy = (double)hy[s] + (double)ly[s];
         double vz = (double)hz[s] + (double)lz[s];
-        if (comb) {
+        if (comb) {  // split tiles hold at most TILE_MAX sinks (host-built)
+            if (j >= TILE_MAX) continue;
             comb->v[wslot][0][j] = vx;
             comb->v[wslot][1][j] = vy;
             comb->v[wslot][2][j] = vz;
@@ -268,8 +300,10 @@ __device__ __forceinline__ void dispatch_tile(const KParams &kp, WarpSmem &ws, c
         run_tile<SOFT, DENS, 1, UNR>(kp, ws, it, lane, comb, wslot);
     else if (SMAX == 2 || it.S == 2)
         run_tile<SOFT, DENS, 2, UNR>(kp, ws, it, lane, comb, wslot);
+    else if (SMAX == 4 || it.S == 4)
+        run_tile<SOFT, DENS, 4, UNR>(kp, ws, it, lane, comb, wslot);
     else
-        run_tile<SOFT, DENS, (SMAX >= 4 ? 4 : 2), UNR>(kp, ws, it, lane, comb, wslot);
+        run_tile<SOFT, DENS, (SMAX >= 8 ? 8 : 4), UNR>(kp, ws, it, lane, comb, wslot);
 }
 
 // The persistent pencil kernel.  Shape knobs (chosen by the autotuner):
@@ -365,7 +399,7 @@ struct Variant {
 static const Variant VARIANTS[] = {
     {4, 8, 2, "sinks/lane<=4 unroll 8, 2 CTAs/SM"},
     {4, 4, 2, "sinks/lane<=4 unroll 4, 2 CTAs/SM"},
-    {4, 4, 3, "sinks/lane<=4 unroll 4, 3 CTAs/SM"},
+    {8, 4, 1, "sinks/lane<=8 unroll 4, 1 CTA/SM"},
     {2, 8, 3, "sinks/lane<=2 unroll 8, 3 CTAs/SM"},
     {2, 4, 4, "sinks/lane<=2 unroll 4, 4 CTAs/SM"},
 };
@@ -375,7 +409,7 @@ template <int SOFT, bool DENS>
 static KernelFn variant_kernel(int v) {
     switch (v) {
     case 1: return pencil_kernel<SOFT, DENS, 4, 4, 2>;
-    case 2: return pencil_kernel<SOFT, DENS, 4, 4, 3>;
+    case 2: return pencil_kernel<SOFT, DENS, 8, 4, 1>;
     case 3: return pencil_kernel<SOFT, DENS, 2, 8, 3>;
     case 4: return pencil_kernel<SOFT, DENS, 2, 4, 4>;
     default: return pencil_kernel<SOFT, DENS, 4, 8, 2>;
@@ -477,11 +511,13 @@ static nf_status build_plan(nf_ctx *ctx, nf_box *box, int lo, int hi, int varian
                     if (forced_S)
                         S = std::min(forced_S, smax);
                     else
-                        S = rem <= 32 ? 1 : (rem <= 64 || smax == 2 ? 2 : 4);
+                        S = rem <= 32 ? 1
+                            : (rem <= 64 || smax == 2) ? 2
+                            : (rem <= 128 || smax == 4) ? 4 : 8;
                     int take = (int)std::min<int64_t>(rem, 32 * S);
                     HostTile t;
                     t.it = Item{pencil, (int)done, take, S, 0, (int)M, 0, 0};
-                    int64_t Mpad = (M / 32) * 32 + ((M % 32) + unr - 1) / unr * unr;
+                    int64_t Mpad = (M / CHUNK) * CHUNK + ((M % CHUNK) + unr - 1) / unr * unr;
                     t.cost = (double)(32 * S) * (double)Mpad + 2000.0 * S;
                     pairs += (uint64_t)take * (uint64_t)M;
                     padded += (uint64_t)(32 * S) * (uint64_t)Mpad;
@@ -506,10 +542,25 @@ static nf_status build_plan(nf_ctx *ctx, nf_box *box, int lo, int hi, int varian
     double thr = total / (2.0 * pl.warps);
     std::vector<HostTile> heavy, light;
     for (auto &t : tiles) {
-        if (t.cost > thr && t.it.src_end >= 64 * WARPS_PER_CTA)
-            heavy.push_back(t);
-        else
+        if (t.cost > thr && t.it.src_end >= 64 * WARPS_PER_CTA) {
+            // split tiles are summed through shared memory sized for
+            // TILE_MAX sinks: halve larger tiles first
+            if (t.it.nsink > TILE_MAX) {
+                HostTile a = t, b = t;
+                a.it.S = b.it.S = 4;
+                a.it.nsink = TILE_MAX;
+                b.it.sink_begin += TILE_MAX;
+                b.it.nsink = t.it.nsink - TILE_MAX;
+                if (b.it.nsink <= 64) b.it.S = b.it.nsink <= 32 ? 1 : 2;
+                a.cost = b.cost = t.cost / 2;
+                heavy.push_back(a);
+                heavy.push_back(b);
+            } else {
+                heavy.push_back(t);
+            }
+        } else {
             light.push_back(t);
+        }
     }
     auto by_cost = [](const HostTile &a, const HostTile &b) {
         if (a.cost != b.cost) return a.cost > b.cost;
@@ -522,7 +573,7 @@ static nf_status build_plan(nf_ctx *ctx, nf_box *box, int lo, int hi, int varian
     hv.reserve(heavy.size() * WARPS_PER_CTA);
     for (auto &t : heavy) {
         int M = t.it.src_end;
-        int per = ((M + WARPS_PER_CTA - 1) / WARPS_PER_CTA + 31) / 32 * 32;
+        int per = ((M + WARPS_PER_CTA - 1) / WARPS_PER_CTA + CHUNK - 1) / CHUNK * CHUNK;
         for (int w = 0; w < WARPS_PER_CTA; w++) {
             Item it = t.it;
             it.src_begin = std::min(M, w * per);
@@ -588,6 +639,15 @@ static KParams params_from(nf_ctx *ctx, const EngineLaunch &L) {
         kp.pc.c1 = (float)(-15.0 * ie2 * ie2);
         kp.pc.c2 = (float)(6.0 * pow(ie2, 2.5));
         kp.pc.c3 = (float)(10.0 * pow(ie2, 1.5));
+    }
+    {
+        // face slabs of width eps (+1% and a rounding allowance) on either
+        // side of the pencil column, in a source cell's own frame
+        double h = 1.0 / (double)L.cpd;
+        double e = cfg.softening == SOFT_SINGLE_SPLINE ? 1.0 / sqrt((double)cfg.eps) : 0.0;
+        double w = e * 1.01 + 1e-6 * h;
+        kp.face_lo = (float)(-0.5 * h + w);
+        kp.face_hi = (float)(0.5 * h - w);
     }
     double h = 1.0 / (double)L.cpd;
     for (int a = 0; a < 2 * R + 1; a++) {
@@ -927,6 +987,17 @@ static nf_status get_plan(nf_ctx *ctx, nf_box *box, int lo, int hi, Plan **out) 
     *out = pl.get();
     box->plans[key] = std::move(pl);
     return NF_OK;
+}
+
+// The cached plan of a slab range (built, and the box tuned, on first use),
+// for launches that bring their own partials, counters and output (serving).
+nf_status nf::box_plan(nf_ctx *ctx, nf_box *box, int lo, int hi, const Plan **out) {
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    NF_CUDA(cudaSetDevice(ctx->device));
+    Plan *pl = nullptr;
+    nf_status st = get_plan(ctx, box, lo, hi, &pl);
+    *out = pl;
+    return st;
 }
 
 extern "C" int nf_kernel_variant_count(void) { return NVARIANTS; }

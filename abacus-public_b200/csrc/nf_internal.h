@@ -82,6 +82,12 @@ int engine_plain_variant();
 constexpr int ENGINE_WARPS_PER_CTA = 8;
 // SIC size limits from a buffer budget (the reference's bytes-per-block model).
 nf_status sic_limits(int out_kind, int cpd, uint64_t max_buffer_bytes, nf_gpu_limits *lim);
+// The cached work list of a box's slab range (nf_box.cu).
+struct Plan;
+}  // namespace nf
+struct nf_box;
+namespace nf {
+nf_status box_plan(nf_ctx *ctx, nf_box *box, int lo, int hi, const Plan **out);
 
 }  // namespace nf
 

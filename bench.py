@@ -151,12 +151,18 @@ def dist_init(n_gpus):
     return rank, world, local
 
 
+def _reduce_device():
+    import torch.distributed as dist
+    return "cuda" if dist.get_backend() == "nccl" else "cpu"
+
+
 def barrier_max(value: float, world: int) -> float:
+    """Max over ranks (the timed region's duration is the slowest rank's)."""
     if world == 1:
         return value
     import torch
     import torch.distributed as dist
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    t = torch.tensor([value], dtype=torch.float64, device=_reduce_device())
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -172,9 +178,21 @@ def all_sum(value: float, world: int) -> float:
         return value
     import torch
     import torch.distributed as dist
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    t = torch.tensor([value], dtype=torch.float64, device=_reduce_device())
     dist.all_reduce(t, op=dist.ReduceOp.SUM)
     return float(t.item())
+
+
+def rank_seed_offset(rank: int) -> int:
+    """Each rank sweeps its own independent box: seed + rank."""
+    return rank
+
+
+def aggregate(pairs_per_rank: float, ms_per_rank: float, world: int) -> tuple[float, float]:
+    """Whole-job pairs/s: all ranks' pairs over the slowest rank's time."""
+    total = all_sum(pairs_per_rank, world)
+    ms = barrier_max(ms_per_rank, world)
+    return total / (ms / 1e3), ms
 
 
 # ---------------------------------------------------------------------------
@@ -291,12 +309,92 @@ def percentile(xs, q):
     return float(np.percentile(np.asarray(xs), q)) if xs else None
 
 
+def plain_dropin(capi, box, w, device, steps=2):
+    """Pairs/s of the plain drop-in: the NearFieldDriver mirror (SIC planning,
+    y-splits, one launch per SIC, host slabs staged per SIC, AccSlab written
+    back) over every slab of the box; wall clock per full sweep."""
+    from abacus_public_b200 import synth
+    length = synth.plummer_eps(w["n_side"])
+    drv = capi.Driver(box, softening=w["softening"], softening_length=length, device=device,
+                      direct_bpd=3)
+    try:
+        drv.run_all()  # warm-up: buffers, pinned staging
+        times = []
+        for _ in range(steps):
+            t0 = time.perf_counter()
+            drv.run_all()
+            times.append(time.perf_counter() - t0)
+        st = drv.stats()
+        pairs = st.direct_interactions // (steps + 1)
+        sec = float(np.mean(times))
+        return {"value": pairs / sec, "unit": "pairs/s", "ms_per_step": 1e3 * sec,
+                "splits_per_slab": st.mean_splits_per_slab, "buffers": st.nbuffers,
+                "gb_to_device_per_step": st.total_gb_to / (steps + 1),
+                "what": "host slabs -> NearFieldDriver -> SIC -> AccSlab, wall clock"}
+    finally:
+        drv.close()
+
+
+def serving_phase(capi, ctx, db_main, w, args, rank, loads=(0.5, 1.0, 1.5), seed=7):
+    """Seeded Poisson slab requests over the main box and a second clustered
+    box (cpd 45, ~64 per cell) resident on the same GPU, at fractions of the
+    measured closed-loop capacity; p50/p99 latency from submission to the
+    result in the caller's device buffer."""
+    import torch
+    from abacus_public_b200 import synth
+    other = synth.clustered_box(64 * 45 ** 3, 45, seed=100 + rank)
+    db2 = ctx.box(other)
+    dbs = [db_main, db2]
+    slabs = [(i, s) for i, d in enumerate(dbs) for s in range(d.cpd)]
+    outs = {}
+    for i, s in slabs:
+        p0, p1 = dbs[i].slab_particles(s, s + 1)
+        outs[(i, s)] = torch.empty((max(p1 - p0, 1), 4), dtype=torch.float32, device="cuda")
+    rng = np.random.default_rng(seed)
+    per_level = args.serve_requests
+    levels = []
+    with capi.Server(ctx, max_inflight=8) as srv:
+        for _ in range(2):  # warm-up (plans, tuning); the second pass gives capacity
+            t0 = time.perf_counter()
+            tk = [srv.submit(dbs[i], s, outs[(i, s)].data_ptr(), True) for i, s in slabs]
+            for t in tk:
+                srv.wait(t)
+            cap = len(slabs) / (time.perf_counter() - t0)
+        for load in loads:
+            rate = load * cap
+            arr = np.cumsum(rng.exponential(1.0 / rate, per_level))
+            pick = rng.integers(0, len(slabs), per_level)
+            srv.reset_stats()
+            tk = []
+            t_start = time.perf_counter()
+            for k in range(per_level):
+                target = t_start + arr[k]
+                while True:
+                    now = time.perf_counter()
+                    if now >= target:
+                        break
+                    time.sleep(min(target - now, 2e-4))
+                i, s = slabs[pick[k]]
+                tk.append(srv.submit(dbs[i], s, outs[(i, s)].data_ptr(), True))
+            for t in tk:
+                srv.wait(t)
+            elapsed = time.perf_counter() - t_start
+            st = srv.stats()
+            levels.append({"load": load, "rate_per_s": rate, "requests": per_level,
+                           "p50_ms": st.p50_ms, "p99_ms": st.p99_ms, "mean_ms": st.mean_ms,
+                           "queue_p99_ms": st.queue_p99_ms, "pairs_per_s": st.pairs / elapsed,
+                           "max_concurrent": st.max_concurrent})
+    db2.close()
+    return {"boxes": [f"{w['n_side']}^3 cpd {db_main.cpd}", "64*45^3 cpd 45 clustered"],
+            "capacity_slabs_per_s": cap, "levels": levels}
+
+
 def our_arm(args, w):
     import torch
     rank, world, local = dist_init(args.gpus)
     _pkg()
     from abacus_public_b200 import capi
-    box = make_box(w, seed_offset=rank)
+    box = make_box(w, seed_offset=rank_seed_offset(rank))
     eps = kernel_eps(w)
     soft = w["softening"]
     ctx = capi.Context(softening=soft, eps=eps, device=local)
@@ -367,16 +465,11 @@ def our_arm(args, w):
     e2e_ms = barrier_max(e0.elapsed_time(e1) / args.steps, world)
     e2e_value = total_pairs / (e2e_ms / 1e3)
 
-    # slab latency: one request per x-slab, result in the caller's device buffer
-    lat = []
-    for s in range(box.cpd):
-        p0, p1 = db.slab_particles(s, s + 1)
-        db.forces_device(s, s + 1, out_dev.data_ptr())  # warm the slab's graph
-    for rep in range(2):
-        for s in range(box.cpd):
-            t0 = time.perf_counter()
-            db.forces_device(s, s + 1, out_dev.data_ptr())
-            lat.append(1e3 * (time.perf_counter() - t0))
+    # the plain drop-in on the same box: NearFieldDriver -> SICs from host slabs
+    plain = None if args.no_plain else plain_dropin(capi, box, w, local, steps=2)
+    # serving: seeded Poisson slab requests over this box and a second one
+    serving = serving_phase(capi, ctx, db, w, args, rank)
+    lvl1 = [v for v in serving["levels"] if v["load"] == 1.0][0]
 
     tv, tms = db.tuning()
     lib = capi.lib()
@@ -404,9 +497,13 @@ def our_arm(args, w):
                    "accumulation": "compensated",
                    "l2": "inputs larger than L2 (positions 16 B x N + 120 B x N partials)",
                    "parallelism": f"independent boxes x{world}"},
-        "slab_latency_ms": {"p50": percentile(lat, 50), "p99": percentile(lat, 99),
-                            "n": len(lat), "what": "one x-slab request, call to result in "
-                                                  "the caller's device buffer"},
+        "slab_latency_ms": {"p50": lvl1["p50_ms"], "p99": lvl1["p99_ms"],
+                            "n": lvl1["requests"],
+                            "what": "serving at 1.0x measured capacity: Poisson slab requests "
+                                    "over two resident boxes, submit to result in the caller's "
+                                    "device buffer"},
+        "serving": serving,
+        "plain_dropin": plain,
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak_sust, "unit": "TFLOP/s",
                      "frac": achieved / peak_sust, "traffic": traffic,
                      "kernel": "pencil_kernel", "kernel_ms": k_ms,
@@ -450,6 +547,9 @@ def main():
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="clustered256")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain drop-in phase")
+    ap.add_argument("--serve-requests", type=int, default=2000,
+                    help="slab requests per serving load level")
     ap.add_argument("--profile", action="store_true",
                     help="timed sweeps only (no peak probe, CPU baseline, e2e or latency "
                          "phases): the command profiled under ncu")

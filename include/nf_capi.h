@@ -328,6 +328,55 @@ const char *nf_kernel_variant_name(int variant);
  * candidate during tuning (ms[0 .. n-1]). */
 nf_status nf_box_tuning(const nf_box *box, int *variant, float *ms, int n);
 
+/* ---------------- 4. serving: slab requests over resident boxes ---------------- */
+/* A request loop with continuous admission: slab requests (one x-slab of
+ * one registered box) may be submitted from any thread at any time; a
+ * dispatcher admits them, oldest first, as soon as a slot is free and the
+ * request's device memory fits the HBM budget, and launches each on its own
+ * stream, so requests that arrive while others run overlap with them on the
+ * device.  Positions stay resident (nf_box_create); each admitted request
+ * holds its own partials, counters and output until it completes.  The
+ * result goes to the caller's buffer (host or device); latency is measured
+ * from submission to the result being there. */
+typedef struct nf_server nf_server;
+typedef uint64_t nf_ticket;
+
+typedef struct nf_server_config {
+    size_t hbm_budget_bytes;  /* device bytes admitted requests may hold; 0 = 90% of the
+                                 device memory free when the server starts */
+    int max_inflight;         /* slots: requests on the device at once (default 8) */
+    int max_queued;           /* pending requests beyond which submit fails (default 65536) */
+} nf_server_config;
+
+typedef struct nf_server_stats {
+    uint64_t submitted, admitted, completed, failed, rejected, cancelled;
+    uint64_t pairs;               /* pairs of completed requests */
+    double busy_s;                /* wall time with at least one request admitted */
+    double p50_ms, p99_ms, mean_ms, max_ms;  /* latency: submit -> result in caller's buffer */
+    double queue_p50_ms, queue_p99_ms;       /* submit -> admission */
+    int max_concurrent;           /* most requests on the device at once */
+    size_t hbm_budget_bytes, hbm_peak_bytes;
+} nf_server_stats;
+
+nf_status nf_server_start(nf_ctx *ctx, const nf_server_config *cfg, nf_server **out);
+/* Queue one slab request.  `out` receives the slab's records (particle
+ * order); it must stay valid until the ticket completes.  NF_EADMISSION if
+ * the request alone cannot fit the HBM budget or the queue is full. */
+nf_status nf_server_submit(nf_server *srv, nf_box *box, int slab, void *out, int out_on_device,
+                           nf_ticket *ticket);
+/* *state: 1 completed, 0 pending or running, -1 failed or cancelled. */
+nf_status nf_server_poll(nf_server *srv, nf_ticket ticket, int *state);
+/* Wait for a ticket (bounded): NF_OK, NF_ETIMEDOUT, NF_ECANCELLED or the
+ * request's failure status. */
+nf_status nf_server_wait(nf_server *srv, nf_ticket ticket, uint64_t timeout_ns);
+/* Cancel a request that has not been admitted yet (NF_EINVAL otherwise). */
+nf_status nf_server_cancel(nf_server *srv, nf_ticket ticket);
+nf_status nf_server_stats_get(nf_server *srv, nf_server_stats *stats);
+/* Reset latency statistics (e.g. after warm-up). */
+nf_status nf_server_stats_reset(nf_server *srv);
+/* Drain or cancel what is queued, wait for what runs (bounded), stop. */
+void nf_server_stop(nf_server *srv);
+
 /* Allocation-free variant of the batched sweep (no counterpart in the
  * reference).  For callers that cannot call cudaMalloc -- code that runs
  * inside another framework's memory pool or caching allocator, or in a
