@@ -134,8 +134,17 @@ class ServerStats(ctypes.Structure):
                 ("hbm_peak_bytes", ctypes.c_size_t)]
 
 
+class RequestInfo(ctypes.Structure):
+    _fields_ = [("state", ctypes.c_int), ("status", ctypes.c_int), ("slab", ctypes.c_int),
+                ("slot", ctypes.c_int), ("pairs", ctypes.c_uint64),
+                ("submit_ms", ctypes.c_double), ("queue_ms", ctypes.c_double),
+                ("run_ms", ctypes.c_double), ("total_ms", ctypes.c_double)]
+
+
 # Every symbol the header declares; the loader checks each one is exported.
 EXPORTS = {
+    "nf_server_request_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64,
+                                              ctypes.POINTER(RequestInfo)]),
     "nf_server_start": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ServerConfig),
                                        ctypes.POINTER(ctypes.c_void_p)]),
     "nf_server_submit": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
@@ -497,6 +506,13 @@ class Server:
 
     def cancel(self, ticket: int):
         check(lib().nf_server_cancel(self.h, ticket), "nf_server_cancel")
+
+    def info(self, ticket: int) -> RequestInfo:
+        """The request's record: state, slot, submit time and its latency split."""
+        r = RequestInfo()
+        check(lib().nf_server_request_info(self.h, ticket, ctypes.byref(r)),
+              "nf_server_request_info")
+        return r
 
     def stats(self) -> ServerStats:
         s = ServerStats()

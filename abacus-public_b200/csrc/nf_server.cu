@@ -10,6 +10,13 @@
 // the device (a persistent grid's tail is filled by the next request's
 // CTAs; copies overlap kernels).  A host callback after the copy marks the
 // request complete and frees its slot; latency is submit -> that callback.
+//
+// Slot memory comes from a memory pool owned by the server and is
+// allocated and freed stream-ordered on the slot's stream, so growing one
+// slot never waits for the requests running on the others (a plain
+// cudaFree would synchronise the whole device).  A slot that must grow is
+// sized for the largest slab of the request's box when the budget allows,
+// so each slot grows at most once per box geometry.
 #include <algorithm>
 #include <chrono>
 #include <cstring>
@@ -45,6 +52,8 @@ struct Req {
     sclock::time_point t_submit, t_admit, t_done;
     uint64_t pairs = 0;
     Slot *slot = nullptr;
+    int slot_index = -1;  // the slot it ran on (kept after completion)
+    int waiters = 0;      // threads inside nf_server_wait on this request
     struct nf_server *srv = nullptr;
 };
 
@@ -65,6 +74,9 @@ struct nf_server {
     bool stop = false;
     int running = 0, max_running = 0;
     std::thread dispatcher;
+    cudaMemPool_t pool = nullptr;
+    sclock::time_point t_start;
+    std::deque<nf_ticket> finished;  // retired oldest first beyond NF_SERVER_HISTORY
     // statistics
     uint64_t submitted = 0, admitted = 0, completed = 0, failed = 0, rejected = 0, cancelled = 0;
     uint64_t pairs = 0;
@@ -75,6 +87,24 @@ struct nf_server {
 
 static size_t rec_bytes(const nf_ctx *ctx) { return ctx->cfg.out_kind == NF_OUT_FLOAT4 ? 16 : 12; }
 
+// Finished requests kept for poll/wait/request_info before the oldest are
+// forgotten (their tickets then read as unknown).
+static constexpr size_t NF_SERVER_HISTORY = 1u << 16;
+
+// A request reached a final state (s->mu held): remember it, and forget the
+// oldest finished ones beyond the history bound that nobody waits on.
+static void finish(nf_server *s, Req *r) {
+    s->finished.push_back(r->id);
+    while (s->finished.size() > NF_SERVER_HISTORY) {
+        auto it = s->reqs.find(s->finished.front());
+        if (it != s->reqs.end()) {
+            if (it->second->waiters > 0) break;
+            s->reqs.erase(it);
+        }
+        s->finished.pop_front();
+    }
+}
+
 static void CUDART_CB on_done(void *arg) {
     Req *r = (Req *)arg;
     nf_server *s = r->srv;
@@ -82,6 +112,7 @@ static void CUDART_CB on_done(void *arg) {
         std::lock_guard<std::mutex> lk(s->mu);
         r->t_done = sclock::now();
         r->state = 2;
+        r->slot_index = r->slot->index;
         r->slot->req = nullptr;
         r->slot = nullptr;
         s->completed++;
@@ -90,6 +121,7 @@ static void CUDART_CB on_done(void *arg) {
         s->queue_ms.push_back(std::chrono::duration<double, std::milli>(r->t_admit - r->t_submit).count());
         if (--s->running == 0)
             s->busy_s += std::chrono::duration<double>(r->t_done - s->busy_since).count();
+        finish(s, r);
     }
     s->cv.notify_all();
     s->cv_done.notify_all();
@@ -97,70 +129,104 @@ static void CUDART_CB on_done(void *arg) {
 
 // Booking for one admission: the slot to (re)allocate and idle slots whose
 // buffers are released to stay within the budget.  Decided with s->mu held;
-// the CUDA calls happen after the lock is dropped (cudaFree waits for device
-// work, including host callbacks that take s->mu).
+// the CUDA calls happen after the lock is dropped.
 struct Booking {
     Slot *slot = nullptr;
     size_t part = 0, out = 0;  // new capacities (0: keep the slot's buffers)
     std::vector<Slot *> release;
+    std::vector<void *> release_ptrs;  // their buffers, taken at booking time
 };
 
-static bool book_slot(nf_server *s, Slot &sl, size_t part_need, size_t out_need, Booking &bk) {
-    bk = Booking{};
-    bk.slot = &sl;
-    if (sl.part_cap >= part_need && sl.out_cap >= out_need && sl.counters) return true;
-    size_t gp = std::max(part_need, sl.part_cap), go = std::max(out_need, sl.out_cap);
+// Device bytes of a slab request: partials (one record of nc doubles per
+// sink and pencil slot) and the output records.
+static void request_bytes(const nf_server *s, int64_t nsink, size_t *part, size_t *out) {
+    const int W = 2 * s->ctx->cfg.near_field_radius + 1;
+    const int nc = s->ctx->cfg.b2 > 0.f ? 4 : 3;
+    *part = (size_t)W * nc * (size_t)nsink * sizeof(double) + 16;
+    *out = (size_t)nsink * rec_bytes(s->ctx) + 16;
+}
+
+static int64_t largest_slab(const nf_box *box) {
+    const int64_t c2 = (int64_t)box->cpd * box->cpd;
+    int64_t m = 0;
+    for (int x = 0; x < box->cpd; x++)
+        m = std::max(m, box->cell_start[(x + 1) * c2] - box->cell_start[x * c2]);
+    return m;
+}
+
+// Try to book capacities gp/go for slot sl, releasing idle slots' buffers
+// as needed; false (nothing changed) if the budget cannot hold them.
+static bool try_book(nf_server *s, Slot &sl, size_t gp, size_t go, Booking &bk) {
     size_t held = s->held - sl.bytes() + gp + go + 256;
+    std::vector<Slot *> rel;
     for (auto &o : s->slots) {
         if (held <= s->budget) break;
         if (&o == &sl || o.req || !o.part_cap) continue;
-        bk.release.push_back(&o);
+        rel.push_back(&o);
         held -= o.bytes();
     }
     if (held > s->budget) return false;
     bk.part = gp;
     bk.out = go;
-    for (Slot *o : bk.release) {  // book the new total now
-        s->held -= o->bytes();
+    for (Slot *o : rel) {  // book the new total now; the buffers go back after the unlock
         o->part_cap = o->out_cap = 0;
-    }
-    s->held = s->held - sl.bytes() + gp + go + 256;
-    s->peak = std::max(s->peak, s->held);
-    return true;
-}
-
-// Carry out a booking (no lock held).
-static nf_status apply_booking(Booking &bk) {
-    for (Slot *o : bk.release) {
-        cudaFree(o->part);
-        cudaFree(o->out);
-        cudaFree(o->counters);
+        bk.release.push_back(o);
+        bk.release_ptrs.insert(bk.release_ptrs.end(), {o->part, o->out, o->counters});
         o->part = nullptr;
         o->out = nullptr;
         o->counters = nullptr;
     }
+    s->held = held;
+    s->peak = std::max(s->peak, s->held);
+    sl.part_cap = gp;  // booked; allocated by apply_booking
+    sl.out_cap = go;
+    return true;
+}
+
+static bool book_slot(nf_server *s, Slot &sl, const nf_box *box, size_t part_need,
+                      size_t out_need, Booking &bk) {
+    bk = Booking{};
+    bk.slot = &sl;
+    if (sl.part_cap >= part_need && sl.out_cap >= out_need && sl.counters) return true;
+    // grow to the box's largest slab if the budget allows, else to this request
+    size_t pm, om;
+    request_bytes(s, largest_slab(box), &pm, &om);
+    pm = std::max({pm, part_need, sl.part_cap});
+    om = std::max({om, out_need, sl.out_cap});
+    if (try_book(s, sl, pm, om, bk)) return true;
+    return try_book(s, sl, std::max(part_need, sl.part_cap), std::max(out_need, sl.out_cap), bk);
+}
+
+// Carry out a booking (no lock held): stream-ordered frees and allocations
+// from the server's pool.  The released slots are idle; their buffers are
+// freed on their own streams, behind the work those streams last ran.
+static nf_status apply_booking(nf_server *s, Booking &bk) {
+    for (size_t i = 0; i < bk.release.size(); i++)
+        for (int k = 0; k < 3; k++)
+            if (bk.release_ptrs[3 * i + k]) cudaFreeAsync(bk.release_ptrs[3 * i + k], bk.release[i]->stream);
     if (!bk.part) return NF_OK;
     Slot &sl = *bk.slot;
-    cudaFree(sl.part);
-    cudaFree(sl.out);
-    cudaFree(sl.counters);
+    cudaStream_t st = sl.stream;
+    if (sl.part) cudaFreeAsync(sl.part, st);
+    if (sl.out) cudaFreeAsync(sl.out, st);
+    if (sl.counters) cudaFreeAsync(sl.counters, st);
     sl.part = nullptr;
     sl.out = nullptr;
     sl.counters = nullptr;
-    if (cudaMalloc(&sl.part, bk.part) != cudaSuccess || cudaMalloc(&sl.out, bk.out) != cudaSuccess ||
-        cudaMalloc(&sl.counters, 256) != cudaSuccess) {
+    void *p = nullptr, *o = nullptr, *c = nullptr;
+    cudaError_t e = cudaMallocFromPoolAsync(&p, bk.part, s->pool, st);
+    if (e == cudaSuccess) e = cudaMallocFromPoolAsync(&o, bk.out, s->pool, st);
+    if (e == cudaSuccess) e = cudaMallocFromPoolAsync(&c, 256, s->pool, st);
+    if (e != cudaSuccess) {
         cudaGetLastError();
-        cudaFree(sl.part);
-        cudaFree(sl.out);
-        cudaFree(sl.counters);
-        sl.part = nullptr;
-        sl.out = nullptr;
-        sl.counters = nullptr;
+        for (void *q : {p, o, c})
+            if (q) cudaFreeAsync(q, st);
         set_error("nf_server: device allocation failed within the HBM budget");
         return NF_ENOMEM;
     }
-    sl.part_cap = bk.part;
-    sl.out_cap = bk.out;
+    sl.part = (double *)p;
+    sl.out = o;
+    sl.counters = (int *)c;
     return NF_OK;
 }
 
@@ -205,13 +271,12 @@ static void fail_admitted(nf_server *s, Req *r, Slot *sl, nf_status st) {
     s->failed++;
     if (--s->running == 0)
         s->busy_s += std::chrono::duration<double>(sclock::now() - s->busy_since).count();
+    finish(s, r);
     s->cv_done.notify_all();
 }
 
 static void dispatcher_main(nf_server *s) {
     cudaSetDevice(s->ctx->device);
-    const int W = 2 * s->ctx->cfg.near_field_radius + 1;
-    const int nc = s->ctx->cfg.b2 > 0.f ? 4 : 3;
     std::unique_lock<std::mutex> lk(s->mu);
     for (;;) {
         s->cv.wait(lk, [&] {
@@ -234,22 +299,24 @@ static void dispatcher_main(nf_server *s) {
             r->state = -1;
             r->status = st;
             s->failed++;
+            finish(s, r);
             s->cv_done.notify_all();
             continue;
         }
-        size_t part_need = (size_t)W * nc * (size_t)pl->n_range * sizeof(double) + 16;
-        size_t out_need = (size_t)pl->n_range * rec_bytes(s->ctx) + 16;
+        size_t part_need, out_need;
+        request_bytes(s, pl->n_range, &part_need, &out_need);
         Slot *pick = nullptr;  // a free slot, preferring one already large enough
         for (auto &sl : s->slots)
             if (!sl.req && (!pick || (sl.part_cap >= part_need && pick->part_cap < part_need)))
                 pick = &sl;
         Booking bk;
-        if (!pick || !book_slot(s, *pick, part_need, out_need, bk)) {
+        if (!pick || !book_slot(s, *pick, r->box, part_need, out_need, bk)) {
             if (s->running == 0) {  // nothing in flight will free memory
                 s->pending.pop_front();
                 r->state = -1;
                 r->status = NF_EADMISSION;
                 s->rejected++;
+                finish(s, r);
                 s->cv_done.notify_all();
                 continue;
             }
@@ -266,7 +333,7 @@ static void dispatcher_main(nf_server *s) {
         if (s->running++ == 0) s->busy_since = r->t_admit;
         s->max_running = std::max(s->max_running, s->running);
         lk.unlock();
-        st = apply_booking(bk);
+        st = apply_booking(s, bk);
         if (st == NF_OK) st = launch_request(s, r, *pick, pl);
         lk.lock();
         if (st != NF_OK) fail_admitted(s, r, pick, st);
@@ -292,6 +359,16 @@ extern "C" nf_status nf_server_start(nf_ctx *ctx, const nf_server_config *cfg, n
     size_t freeb = 0, total = 0;
     NF_CUDA(cudaMemGetInfo(&freeb, &total));
     s->budget = s->cfg.hbm_budget_bytes ? s->cfg.hbm_budget_bytes : (size_t)(0.9 * (double)freeb);
+    // the slots' memory pool: freed blocks stay in the pool (up to the
+    // budget) for the next growth instead of going back to the driver
+    cudaMemPoolProps pp{};
+    pp.allocType = cudaMemAllocationTypePinned;
+    pp.location.type = cudaMemLocationTypeDevice;
+    pp.location.id = ctx->device;
+    NF_CUDA(cudaMemPoolCreate(&s->pool, &pp));
+    uint64_t keep = s->budget;
+    cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    s->t_start = sclock::now();
     s->slots.resize(s->cfg.max_inflight);
     for (int i = 0; i < s->cfg.max_inflight; i++) {
         s->slots[i].index = i;
@@ -299,6 +376,7 @@ extern "C" nf_status nf_server_start(nf_ctx *ctx, const nf_server_config *cfg, n
         if (e != cudaSuccess) {
             for (auto &sl : s->slots)
                 if (sl.stream) cudaStreamDestroy(sl.stream);
+            cudaMemPoolDestroy(s->pool);
             return cuda_fail(e, "nf_server_start");
         }
     }
@@ -313,11 +391,10 @@ extern "C" nf_status nf_server_submit(nf_server *s, nf_box *box, int slab, void 
         set_error("nf_server_submit: bad argument");
         return NF_EINVAL;
     }
-    const int W = 2 * s->ctx->cfg.near_field_radius + 1;
-    const int nc = s->ctx->cfg.b2 > 0.f ? 4 : 3;
     int64_t c2 = (int64_t)box->cpd * box->cpd;
-    int64_t n = box->cell_start[(slab + 1) * c2] - box->cell_start[slab * c2];
-    size_t need = (size_t)W * nc * n * sizeof(double) + (size_t)n * rec_bytes(s->ctx) + 512;
+    size_t pb, ob;
+    request_bytes(s, box->cell_start[(slab + 1) * c2] - box->cell_start[slab * c2], &pb, &ob);
+    size_t need = pb + ob + 256;
     std::lock_guard<std::mutex> lk(s->mu);
     s->submitted++;
     if (need > s->budget || (int)s->pending.size() >= s->cfg.max_queued) {
@@ -369,8 +446,10 @@ extern "C" nf_status nf_server_wait(nf_server *s, nf_ticket t, uint64_t timeout_
         return NF_EINVAL;
     }
     Req *r = it->second.get();
+    r->waiters++;  // keeps the record while this thread sleeps
     bool ok = s->cv_done.wait_for(lk, std::chrono::nanoseconds(timeout_ns),
                                   [&] { return r->state == 2 || r->state < 0; });
+    r->waiters--;
     if (!ok) {
         set_error("nf_server_wait: request still pending at the timeout");
         return NF_ETIMEDOUT;
@@ -401,7 +480,37 @@ extern "C" nf_status nf_server_cancel(nf_server *s, nf_ticket t) {
     s->pending.erase(std::remove(s->pending.begin(), s->pending.end(), r), s->pending.end());
     r->state = -2;
     s->cancelled++;
+    finish(s, r);
     s->cv_done.notify_all();
+    return NF_OK;
+}
+
+extern "C" nf_status nf_server_request_info(nf_server *s, nf_ticket t, nf_request_info *info) {
+    if (!s || !info) {
+        set_error("nf_server_request_info: null argument");
+        return NF_EINVAL;
+    }
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->reqs.find(t);
+    if (it == s->reqs.end()) {
+        set_error("nf_server_request_info: unknown ticket");
+        return NF_EINVAL;
+    }
+    const Req *r = it->second.get();
+    auto ms = [](sclock::time_point a, sclock::time_point b) {
+        return std::chrono::duration<double, std::milli>(b - a).count();
+    };
+    memset(info, 0, sizeof(*info));
+    info->state = r->state;
+    info->status = r->status;
+    info->slab = r->slab;
+    info->slot = r->slot ? r->slot->index : r->slot_index;
+    info->pairs = r->pairs;
+    info->submit_ms = ms(s->t_start, r->t_submit);
+    const bool admitted = r->state == 1 || r->state == 2 || (r->state == -1 && r->pairs);
+    info->queue_ms = admitted ? ms(r->t_submit, r->t_admit) : -1.0;
+    info->run_ms = r->state == 2 ? ms(r->t_admit, r->t_done) : -1.0;
+    info->total_ms = r->state == 2 ? ms(r->t_submit, r->t_done) : -1.0;
     return NF_OK;
 }
 
@@ -479,13 +588,12 @@ extern "C" void nf_server_stop(nf_server *s) {
     if (s->dispatcher.joinable()) s->dispatcher.join();
     cudaSetDevice(s->ctx->device);
     for (auto &sl : s->slots) {
-        if (sl.stream) {
-            cudaStreamSynchronize(sl.stream);
-            cudaStreamDestroy(sl.stream);
-        }
-        cudaFree(sl.part);
-        cudaFree(sl.out);
-        cudaFree(sl.counters);
+        if (!sl.stream) continue;
+        for (void *q : {(void *)sl.part, sl.out, (void *)sl.counters})
+            if (q) cudaFreeAsync(q, sl.stream);
+        cudaStreamSynchronize(sl.stream);
+        cudaStreamDestroy(sl.stream);
     }
+    if (s->pool) cudaMemPoolDestroy(s->pool);
     delete s;
 }

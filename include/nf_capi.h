@@ -371,6 +371,19 @@ nf_status nf_server_poll(nf_server *srv, nf_ticket ticket, int *state);
 nf_status nf_server_wait(nf_server *srv, nf_ticket ticket, uint64_t timeout_ns);
 /* Cancel a request that has not been admitted yet (NF_EINVAL otherwise). */
 nf_status nf_server_cancel(nf_server *srv, nf_ticket ticket);
+/* One request's record: what happened to it and when.  Finished requests
+ * stay queryable until 65536 newer ones have finished. */
+typedef struct nf_request_info {
+    int state;          /* 0 queued, 1 running, 2 completed, -1 failed, -2 cancelled */
+    nf_status status;   /* failure status (NF_OK otherwise) */
+    int slab, slot;     /* the slab; the slot it runs / ran on (-1: not admitted) */
+    uint64_t pairs;     /* pairs of the slab (0 until admitted) */
+    double submit_ms;   /* submission time, ms since nf_server_start */
+    double queue_ms;    /* submit -> admission (-1: not admitted) */
+    double run_ms;      /* admission -> result in the caller's buffer (-1: not completed) */
+    double total_ms;    /* submit -> result (-1: not completed) */
+} nf_request_info;
+nf_status nf_server_request_info(nf_server *srv, nf_ticket ticket, nf_request_info *info);
 nf_status nf_server_stats_get(nf_server *srv, nf_server_stats *stats);
 /* Reset latency statistics (e.g. after warm-up). */
 nf_status nf_server_stats_reset(nf_server *srv);

@@ -57,6 +57,7 @@ def test_alone_equals_in_the_mix(capi, synth, two_boxes):
             for t in tickets:
                 srv.wait(t)
             st = srv.stats()
+            infos = [srv.info(t) for t in tickets]
         da.close()
         db_.close()
     mixed = outs[("a", s0)]
@@ -70,6 +71,12 @@ def test_alone_equals_in_the_mix(capi, synth, two_boxes):
     assert st.failed == 0 and st.rejected == 0
     assert st.max_concurrent >= 2  # requests overlapped on the device
     assert 0 < st.p50_ms <= st.p99_ms <= st.max_ms
+    # per-request records: completed, on a valid slot, latency = queue + run
+    for inf in infos:
+        assert inf.state == 2 and inf.status == 0 and 0 <= inf.slot < 6 and inf.pairs > 0
+        assert inf.queue_ms >= 0 and inf.run_ms > 0
+        assert inf.total_ms == pytest.approx(inf.queue_ms + inf.run_ms, abs=1e-6)
+    assert max(i.total_ms for i in infos) <= st.max_ms + 1e-9
 
 
 def test_device_output_and_admission_limits(capi, synth, two_boxes):
@@ -127,6 +134,9 @@ def test_cancel_and_stop(capi, synth, two_boxes):
                     assert e.status == capi.NF_ECANCELLED
             st = srv.stats()
             assert st.cancelled == cancelled and st.completed == 40 - cancelled
+            states = [srv.info(t) for t in tk]
+            assert sum(i.state == -2 for i in states) == cancelled
+            assert all(i.queue_ms == -1.0 and i.slot == -1 for i in states if i.state == -2)
             with pytest.raises(capi.NfError):
                 srv.wait(123456789)  # unknown ticket
         db_.close()
