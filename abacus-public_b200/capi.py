@@ -191,6 +191,7 @@ EXPORTS = {
                                      ctypes.c_void_p, ctypes.c_void_p]),
     "nf_box_destroy": (None, [ctypes.c_void_p, ctypes.c_void_p]),
     "nf_box_device_bytes": (ctypes.c_size_t, [ctypes.c_void_p]),
+    "nf_box_set_eps": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_float]),
     "nf_box_forces": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                                      ctypes.c_int, ctypes.c_void_p, ctypes.c_int]),
     "nf_box_pair_count": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
@@ -349,6 +350,10 @@ class DeviceBox:
         check(lib().nf_box_forces(self.ctx.h, self.h, lo, hi, ctypes.c_void_p(dev_ptr), 1),
               "nf_box_forces")
 
+    def set_eps(self, eps: float):
+        """The box's own softening parameter (nf_config.eps convention; 0 = the context's)."""
+        check(lib().nf_box_set_eps(self.ctx.h, self.h, float(eps)), "nf_box_set_eps")
+
     def pair_count(self, lo: int = 0, hi: int | None = None) -> int:
         hi = self.cpd if hi is None else hi
         v = ctypes.c_uint64(0)
@@ -487,6 +492,7 @@ class Server:
         h = ctypes.c_void_p()
         check(lib().nf_server_start(ctx.h, ctypes.byref(cfg), ctypes.byref(h)), "nf_server_start")
         self.h = h
+        self._held = {}  # ticket -> host output array, kept alive until the ticket is waited on
 
     def submit(self, box: DeviceBox, slab: int, out, out_on_device: bool = False) -> int:
         """Queue slab `slab` of `box`; `out` is a host numpy array or a device pointer."""
@@ -494,6 +500,8 @@ class Server:
         ptr = out if out_on_device else out.ctypes.data
         check(lib().nf_server_submit(self.h, box.h, slab, ctypes.c_void_p(ptr),
                                      int(out_on_device), ctypes.byref(t)), "nf_server_submit")
+        if not out_on_device:
+            self._held[t.value] = out  # the library writes into it until completion
         return t.value
 
     def poll(self, ticket: int) -> int:
@@ -502,7 +510,10 @@ class Server:
         return s.value
 
     def wait(self, ticket: int, timeout_s: float = 120.0):
-        check(lib().nf_server_wait(self.h, ticket, int(timeout_s * 1e9)), "nf_server_wait")
+        st = lib().nf_server_wait(self.h, ticket, int(timeout_s * 1e9))
+        if st != NF_ETIMEDOUT:
+            self._held.pop(ticket, None)  # finished (done, failed or cancelled)
+        check(st, "nf_server_wait")
 
     def cancel(self, ticket: int):
         check(lib().nf_server_cancel(self.h, ticket), "nf_server_cancel")
@@ -524,8 +535,9 @@ class Server:
 
     def close(self):
         if self.h:
-            lib().nf_server_stop(self.h)
+            lib().nf_server_stop(self.h)  # waits for what runs: the held arrays are free after
             self.h = None
+            self._held.clear()
 
     def __enter__(self):
         return self

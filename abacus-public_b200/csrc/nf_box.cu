@@ -630,10 +630,11 @@ static KParams params_from(nf_ctx *ctx, const EngineLaunch &L) {
     kp.n_range = L.n_range;
     kp.nc = cfg.b2 > 0.f ? 4 : 3;
     kp.plain = cfg.accumulation == NF_ACC_PLAIN;
-    kp.pc.eps = cfg.eps;
+    const float eps = L.eps > 0.f ? L.eps : cfg.eps;
+    kp.pc.eps = eps;
     kp.pc.b2 = cfg.b2;
     if (cfg.softening == SOFT_SINGLE_SPLINE) {
-        double ie2 = (double)cfg.eps;  // eps_int^-2
+        double ie2 = (double)eps;  // eps_int^-2
         kp.pc.near_thr = (float)(1.0 / ie2);
         kp.pc.inv_eps3 = (float)pow(ie2, 1.5);
         kp.pc.c1 = (float)(-15.0 * ie2 * ie2);
@@ -644,7 +645,7 @@ static KParams params_from(nf_ctx *ctx, const EngineLaunch &L) {
         // face slabs of width eps (+1% and a rounding allowance) on either
         // side of the pencil column, in a source cell's own frame
         double h = 1.0 / (double)L.cpd;
-        double e = cfg.softening == SOFT_SINGLE_SPLINE ? 1.0 / sqrt((double)cfg.eps) : 0.0;
+        double e = cfg.softening == SOFT_SINGLE_SPLINE ? 1.0 / sqrt((double)eps) : 0.0;
         double w = e * 1.01 + 1e-6 * h;
         kp.face_lo = (float)(-0.5 * h + w);
         kp.face_hi = (float)(0.5 * h - w);
@@ -672,11 +673,14 @@ static KParams make_params(nf_ctx *ctx, nf_box *box, const Plan &pl) {
     L.p0 = pl.p0;
     L.n_range = pl.n_range;
     L.variant = pl.variant;
+    L.eps = box->eps;
     return params_from(ctx, L);
 }
 
-static double output_scale(const nf_config &cfg) {
-    if (cfg.softening == SOFT_SINGLE_SPLINE) return pow((double)cfg.eps, -1.5);  // eps_int^3
+// eps: the softening parameter in use (0: the context's)
+static double output_scale(const nf_config &cfg, float eps = 0.f) {
+    if (eps <= 0.f) eps = cfg.eps;
+    if (cfg.softening == SOFT_SINGLE_SPLINE) return pow((double)eps, -1.5);  // eps_int^3
     return 1.0;
 }
 
@@ -710,11 +714,12 @@ nf_status engine_launch(nf_ctx *ctx, const EngineLaunch &L, double, cudaStream_t
     return NF_OK;
 }
 
-nf_status engine_coadd(nf_ctx *ctx, const double *part, int64_t n, void *out, cudaStream_t st) {
+nf_status engine_coadd(nf_ctx *ctx, const double *part, int64_t n, void *out, cudaStream_t st,
+                       float eps) {
     if (n <= 0) return NF_OK;
     const nf_config &cfg = ctx->cfg;
     coadd_kernel<<<ctx->sms * 8, 256, 0, st>>>(part, n, 2 * cfg.near_field_radius + 1,
-                                              cfg.b2 > 0.f ? 4 : 3, output_scale(cfg),
+                                              cfg.b2 > 0.f ? 4 : 3, output_scale(cfg, eps),
                                               cfg.out_kind, out);
     NF_CUDA(cudaGetLastError());
     return NF_OK;
@@ -743,7 +748,7 @@ static nf_status enqueue_forces(nf_ctx *ctx, nf_box *box, Plan &pl, cudaStream_t
     if (pl.n_range > 0) {
         int W = 2 * cfg.near_field_radius + 1;
         int blocks = ctx->sms * 8;
-        coadd_kernel<<<blocks, 256, 0, st>>>(box->d_part, pl.n_range, W, kp.nc, output_scale(cfg),
+        coadd_kernel<<<blocks, 256, 0, st>>>(box->d_part, pl.n_range, W, kp.nc, output_scale(cfg, box->eps),
                                             cfg.out_kind, pl.d_out);
         NF_CUDA(cudaGetLastError());
     }
@@ -852,6 +857,23 @@ extern "C" void nf_box_destroy(nf_ctx *ctx, nf_box *box) {
     cudaFree(box->d_part);
     cudaFree(box->d_stage);
     delete box;
+}
+
+extern "C" nf_status nf_box_set_eps(nf_ctx *ctx, nf_box *box, float eps) {
+    if (!ctx || !box || !(eps >= 0.f) || !std::isfinite(eps)) {
+        set_error("nf_box_set_eps: bad argument (eps must be finite and >= 0)");
+        return NF_EINVAL;
+    }
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    NF_CUDA(cudaSetDevice(ctx->device));
+    if (eps == box->eps) return NF_OK;
+    // cached plans hold graphs with the old constants: wait for every launch
+    // that may use them, then drop them (the kernel-shape choice is kept)
+    NF_CUDA(cudaDeviceSynchronize());
+    for (auto &kv : box->plans) free_plan(*kv.second);
+    box->plans.clear();
+    box->eps = eps;
+    return NF_OK;
 }
 
 extern "C" size_t nf_box_device_bytes(const nf_box *box) { return box ? box->device_bytes() : 0; }

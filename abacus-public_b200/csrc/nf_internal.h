@@ -71,9 +71,11 @@ struct EngineLaunch {
     int64_t p0 = 0, n_range = 0;  // the sinks' particle range
     int variant = 0;
     int grid = 0;                 // CTAs (0: one full wave)
+    float eps = 0.f;              // softening parameter (0: the context's)
 };
 nf_status engine_launch(nf_ctx *ctx, const EngineLaunch &L, double box_h, cudaStream_t st);
-nf_status engine_coadd(nf_ctx *ctx, const double *part, int64_t n, void *out, cudaStream_t st);
+nf_status engine_coadd(nf_ctx *ctx, const double *part, int64_t n, void *out, cudaStream_t st,
+                       float eps = 0.f);
 nf_status engine_pack(nf_ctx *ctx, const float *x, const float *y, const float *z, int64_t n,
                       float4 *out, cudaStream_t st);
 int engine_grid(nf_ctx *ctx, int variant);
@@ -102,6 +104,7 @@ struct nf_box {
     size_t part_bytes = 0;
     std::map<std::pair<int, int>, std::unique_ptr<nf::Plan>> plans;
     int variant = -1;       // kernel shape chosen by the autotuner (-1: not tuned yet)
+    float eps = 0.f;        // the box's own softening parameter (0: the context's)
     float tune_ms[8] = {};  // kernel time of each candidate during tuning
     size_t device_bytes() const;
 };

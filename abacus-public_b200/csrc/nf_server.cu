@@ -246,8 +246,9 @@ static nf_status launch_request(nf_server *s, Req *r, Slot &sl, const Plan *pl) 
     L.n_range = pl->n_range;
     L.variant = pl->variant;
     L.grid = pl->grid;
+    L.eps = r->box->eps;
     nf_status st = engine_launch(ctx, L, 0.0, sl.stream);
-    if (st == NF_OK) st = engine_coadd(ctx, sl.part, pl->n_range, sl.out, sl.stream);
+    if (st == NF_OK) st = engine_coadd(ctx, sl.part, pl->n_range, sl.out, sl.stream, r->box->eps);
     if (st != NF_OK) return st;
     size_t bytes = (size_t)pl->n_range * rec_bytes(ctx);
     if (bytes)

@@ -336,15 +336,29 @@ def plain_dropin(capi, box, w, device, steps=2):
 
 
 def serving_phase(capi, ctx, db_main, w, args, rank, loads=(0.5, 1.0, 1.5), seed=7):
-    """Seeded Poisson slab requests over the main box and a second clustered
-    box (cpd 45, ~64 per cell) resident on the same GPU, at fractions of the
-    measured closed-loop capacity; p50/p99 latency from submission to the
-    result in the caller's device buffer."""
+    """Seeded Poisson slab requests over several boxes resident on the same
+    GPU, at fractions of the measured closed-loop capacity; p50/p99 latency
+    from submission to the result in the caller's device buffer.  Boxes: the
+    main box and a clustered 64*45^3 box, or (`--serve-boxes 45,65,...`)
+    clustered boxes of N = 64*cpd^3 for each listed cpd, each with its own
+    softening at 1/40 of its mean spacing."""
     import torch
     from abacus_public_b200 import synth
-    other = synth.clustered_box(64 * 45 ** 3, 45, seed=100 + rank)
-    db2 = ctx.box(other)
-    dbs = [db_main, db2]
+    soft = w["softening"]
+    own = []
+    if args.serve_boxes:
+        cpds = [int(c) for c in args.serve_boxes.split(",")]
+        dbs, names = [], []
+    else:
+        cpds = [45]
+        dbs, names = [db_main], [f"{w['n_side']}^3 cpd {db_main.cpd}"]
+    for k, c in enumerate(cpds):
+        other = synth.clustered_box(64 * c ** 3, c, seed=100 + 17 * k + rank)
+        d = ctx.box(other)
+        d.set_eps(synth.kernel_eps(soft, synth.plummer_eps(4 * c)))  # 64 per cell: spacing h/4
+        own.append(d)
+        dbs.append(d)
+        names.append(f"64*{c}^3 cpd {c} clustered")
     slabs = [(i, s) for i, d in enumerate(dbs) for s in range(d.cpd)]
     outs = {}
     for i, s in slabs:
@@ -384,9 +398,51 @@ def serving_phase(capi, ctx, db_main, w, args, rank, loads=(0.5, 1.0, 1.5), seed
                            "p50_ms": st.p50_ms, "p99_ms": st.p99_ms, "mean_ms": st.mean_ms,
                            "queue_p99_ms": st.queue_p99_ms, "pairs_per_s": st.pairs / elapsed,
                            "max_concurrent": st.max_concurrent})
-    db2.close()
-    return {"boxes": [f"{w['n_side']}^3 cpd {db_main.cpd}", "64*45^3 cpd 45 clustered"],
-            "capacity_slabs_per_s": cap, "levels": levels}
+    for d in own:
+        d.close()
+    return {"boxes": names, "capacity_slabs_per_s": cap, "levels": levels}
+
+
+def precision_study(capi, box, w, device, stream, steps, comp_out, frac=1e-3, seed=11):
+    """Compensated vs plain FP32 accumulation on the same box: the plain
+    form's sweep rate (device time, positions resident) and both results'
+    RMS / max fractional error against the FP64 oracle on a seeded subsample
+    of `frac` of the sinks.  `comp_out` is the compensated sweep's result."""
+    import torch
+    soft, eps = w["softening"], kernel_eps(w)
+    ctx = capi.Context(softening=soft, eps=eps, device=device, accumulation=capi.ACC_PLAIN)
+    ctx.set_stream(stream.cuda_stream)
+    db = ctx.box(box)
+    out = torch.empty((box.n, 4), dtype=torch.float32, device=f"cuda:{device}")
+    for _ in range(2):
+        db.forces_device(0, box.cpd, out.data_ptr())
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        db.forces_device(0, box.cpd, out.data_ptr())
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    pairs = db.pair_count()
+    plain_out = out.cpu().numpy()
+    db.close()
+    ctx.close()
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+    k = max(2000, int(frac * box.n))
+    sinks = np.sort(np.random.default_rng(seed).choice(box.n, k, replace=False))
+    t0 = time.perf_counter()
+    ref = oracle.fp64_sinks(box, soft, eps, sinks)
+    t_ref = time.perf_counter() - t0
+    res = {"sinks": k, "fp64_oracle_s": t_ref, "plain_pairs_per_s": pairs / (ms / 1e3),
+           "plain_ms_per_step": ms}
+    mag = np.linalg.norm(ref, axis=1)
+    res["small_force_sinks"] = int((mag < 1e-3 * np.median(mag)).sum())  # |a64| < 1e-3 median
+    for name, a in (("compensated", comp_out), ("plain", plain_out)):
+        rms, mx, _ = oracle.frac_errors(a[sinks, :3], ref)
+        res[name] = {"rms_frac": rms, "max_frac": mx}
+    return res
 
 
 def our_arm(args, w):
@@ -468,8 +524,12 @@ def our_arm(args, w):
     # the plain drop-in on the same box: NearFieldDriver -> SICs from host slabs
     plain = None if args.no_plain else plain_dropin(capi, box, w, local, steps=2)
     # serving: seeded Poisson slab requests over this box and a second one
-    serving = serving_phase(capi, ctx, db, w, args, rank)
-    lvl1 = [v for v in serving["levels"] if v["load"] == 1.0][0]
+    serving = None if args.no_serving else serving_phase(capi, ctx, db, w, args, rank)
+    lvl1 = None if serving is None else [v for v in serving["levels"] if v["load"] == 1.0][0]
+    # compensated vs plain accumulation against the FP64 oracle (0.1% of the sinks)
+    precision = None
+    if args.precision_study and rank == 0:
+        precision = precision_study(capi, box, w, local, stream, args.steps, oa)
 
     tv, tms = db.tuning()
     lib = capi.lib()
@@ -497,12 +557,12 @@ def our_arm(args, w):
                    "accumulation": "compensated",
                    "l2": "inputs larger than L2 (positions 16 B x N + 120 B x N partials)",
                    "parallelism": f"independent boxes x{world}"},
-        "slab_latency_ms": {"p50": lvl1["p50_ms"], "p99": lvl1["p99_ms"],
-                            "n": lvl1["requests"],
-                            "what": "serving at 1.0x measured capacity: Poisson slab requests "
-                                    "over two resident boxes, submit to result in the caller's "
-                                    "device buffer"},
+        "slab_latency_ms": None if lvl1 is None else {
+            "p50": lvl1["p50_ms"], "p99": lvl1["p99_ms"], "n": lvl1["requests"],
+            "what": "serving at 1.0x measured capacity: Poisson slab requests over two "
+                    "resident boxes, submit to result in the caller's device buffer"},
         "serving": serving,
+        "precision": precision,
         "plain_dropin": plain,
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak_sust, "unit": "TFLOP/s",
                      "frac": achieved / peak_sust, "traffic": traffic,
@@ -550,6 +610,13 @@ def main():
     ap.add_argument("--no-plain", action="store_true", help="skip the plain drop-in phase")
     ap.add_argument("--serve-requests", type=int, default=2000,
                     help="slab requests per serving load level")
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving phase")
+    ap.add_argument("--serve-boxes", default="",
+                    help="serve clustered boxes of N=64*cpd^3 for these cpds (comma list) "
+                         "instead of the main box + a cpd-45 box")
+    ap.add_argument("--precision-study", action="store_true",
+                    help="also sweep with plain FP32 accumulation and compare both with the "
+                         "FP64 oracle on 0.1%% of the sinks")
     ap.add_argument("--profile", action="store_true",
                     help="timed sweeps only (no peak probe, CPU baseline, e2e or latency "
                          "phases): the command profiled under ncu")

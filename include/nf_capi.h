@@ -30,7 +30,7 @@
  *
  *  3. Batched / serving form: a box whose positions stay resident in HBM
  *     (nf_box_*), one persistent launch per slab range, and a continuous-
- *     batching request loop (nf_serve_*).  These replace
+ *     batching request loop (nf_server_*).  These replace
  *     NearFieldDriver::ExecuteSlab / SlabDone
  *     (singlestep/Timestep/directdriver.cpp:242-431) for callers that keep
  *     positions on the device.
@@ -290,6 +290,12 @@ nf_status nf_box_create(nf_ctx *ctx, int cpd, int64_t np, const int64_t *cell_st
 nf_status nf_box_update(nf_ctx *ctx, nf_box *box, const float *x, const float *y,
                         const float *z);
 void nf_box_destroy(nf_ctx *ctx, nf_box *box);
+/* Give the box its own softening parameter (same convention as
+ * nf_config.eps for the context's softening; 0 = the context's), so that
+ * boxes of different particle spacing share one context and one server.
+ * Waits for the device and drops the box's cached plans: call it while no
+ * sweep or request of this box is in flight. */
+nf_status nf_box_set_eps(nf_ctx *ctx, nf_box *box, float eps);
 /* Device bytes held by the box (positions + plans + partial buffers). */
 size_t nf_box_device_bytes(const nf_box *box);
 

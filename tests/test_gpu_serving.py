@@ -140,3 +140,38 @@ def test_cancel_and_stop(capi, synth, two_boxes):
             with pytest.raises(capi.NfError):
                 srv.wait(123456789)  # unknown ticket
         db_.close()
+
+
+def test_per_box_softening(capi, synth, two_boxes):
+    """Boxes of different spacing under one context and one server: a box
+    given its own eps (nf_box_set_eps) computes exactly what a context with
+    that eps computes, in sweeps and in served slab requests."""
+    boxa, boxb = two_boxes
+    eps_a = synth.kernel_eps(1, synth.plummer_eps(40))
+    eps_b = synth.kernel_eps(1, synth.plummer_eps(45))
+    with capi.Context(softening=1, eps=eps_b, kernel_variant=0) as ctx_b:
+        db_only = ctx_b.box(boxb)
+        want = db_only.forces()
+        # single-slab plans (what the server runs) sum in their own fixed order
+        want_slabs = np.concatenate([db_only.forces(s, s + 1) for s in range(boxb.cpd)])
+        db_only.close()
+    with capi.Context(softening=1, eps=eps_a, kernel_variant=0) as ctx:
+        da, db_ = ctx.box(boxa), ctx.box(boxb)
+        before = db_.forces()  # with the context's eps: differs
+        db_.set_eps(eps_b)
+        got = db_.forces()
+        with capi.Server(ctx, max_inflight=4) as srv:
+            outs = [_slab_out(db_, s) for s in range(boxb.cpd)]
+            tk = [srv.submit(db_, s, outs[s]) for s in range(boxb.cpd)]
+            tka = srv.submit(da, 2, _slab_out(da, 2))
+            for t in tk + [tka]:
+                srv.wait(t)
+        with pytest.raises(capi.NfError):
+            db_.set_eps(float("nan"))
+        da.close()
+        db_.close()
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+    assert not np.array_equal(before, want)
+    served = np.concatenate(outs)
+    assert np.array_equal(served.view(np.uint32), want_slabs.view(np.uint32))
+    np.testing.assert_allclose(served, want, rtol=0, atol=2e-6 * np.abs(want).max())
