@@ -14,13 +14,20 @@
 //
 // One warp runs one tile: up to 32*S sinks of one pencil (S sinks per lane,
 // kept in registers) against the pencil's source stream -- the 25 source
-// cells concatenated, staged 32 at a time into the warp's shared-memory slot
+// cells concatenated, staged 64 at a time into the warp's shared-memory slot
 // from float4 HBM records (register prefetch of the next chunk overlaps the
-// current chunk's math), each source read by every lane with one broadcast
-// LDS.128.  Per chunk the FP32 partial is added to a running partial that is
-// folded into a TwoSum (hi, lo) pair every 64 sources.  A tile writes one
-// double partial per sink and component into the sink's pencil slot; the
-// co-add kernel sums the 2R+1 slots in a fixed order.
+// current chunk's math), each source read by every lane with broadcast
+// loads.  A lane evaluates its sinks two at a time with sm_100's paired FP32
+// instructions (f32x2).  Per 64-source chunk the FP32 partial is folded into
+// a TwoSum (hi, lo) pair.  A tile writes one double partial per sink and
+// component into the sink's pencil slot; the co-add kernel sums the 2R+1
+// slots in a fixed order.
+//
+// Resident boxes are stored with the particles of each cell in Morton order
+// of their cell-relative position (the co-add writes results back in the
+// caller's order): consecutive sinks of a tile then cover a compact region,
+// and for the single spline only the sources within eps of the tile's sink
+// bounding box need the near branch (decided per 32 sources by a warp vote).
 //
 // Scheduling: the host builds a work list per slab range, ordered longest
 // first (LPT).  Tiles whose cost exceeds a share of the launch are split
@@ -31,6 +38,8 @@
 #include <cmath>
 #include <cstring>
 #include <numeric>
+
+#include <cub/device/device_radix_sort.cuh>
 
 #include "nf_internal.h"
 #include "nf_pair.cuh"
@@ -61,21 +70,24 @@ struct KParams {
     float xyshift[MAXW];  // n h, n = -R .. R
     signed char odx[MAXSRC], ody[MAXSRC];  // source cell order: outer ring first
     int n_outer;                           // cells with max(|dx|,|dy|) == 2
-    // single spline: a source in a cell adjacent to the pencil's column can
-    // be closer than eps to one of the pencil's sinks only if it lies within
-    // eps of the shared face, i.e. (own-cell frame) x < face_lo for dx = +1,
-    // x > face_hi for dx = -1 (likewise y)
-    float face_lo, face_hi;
+    // single spline: a source can be closer than eps to one of a tile's
+    // sinks only if it lies within near_w (eps plus a rounding allowance) of
+    // the tile's sink bounding box
+    float near_w;
 };
 
 constexpr int CHUNK = 64;  // sources staged per chunk (two per lane)
 
+// Staged sources are stored negated and duplicated: (-x, -x, -y, -y) and
+// (-z, -z).  A lane then forms sink - source for two of its sinks with one
+// paired add, and every lane reads a source with two broadcast loads.
 struct WarpSmem {
-    float4 buf[CHUNK];
+    float4 bxy[CHUNK];
+    float2 bz[CHUNK];
     int64_t cstart[MAXSRC];
     int32_t cpre[MAXSRC + 1];
     float csx[MAXSRC], csy[MAXSRC];
-    float4 cnear[MAXSRC];  // per source cell: x range, y range of near-capable sources
+    float4 tbb;  // the tile's sink x and y range widened by near_w (single spline)
     int64_t sstart[MAXW];
     int32_t spre[MAXW + 1];
 };
@@ -107,16 +119,6 @@ __device__ void setup_tables(const KParams &kp, const Item &it, WarpSmem &ws, in
         ws.cstart[lane] = st;
         ws.csx[lane] = kp.xyshift[dx + R];
         ws.csy[lane] = kp.xyshift[dy + R];
-        // near-capable ranges: everything for dx = 0, the face slab for
-        // |dx| = 1, nothing for |dx| = 2 (empty range)
-        const float INF = 3.0e38f;
-        float xl = -INF, xh = INF, yl = -INF, yh = INF;
-        if (dx == 1) xh = kp.face_lo;
-        if (dx == -1) xl = kp.face_hi;
-        if (dy == 1) yh = kp.face_lo;
-        if (dy == -1) yl = kp.face_hi;
-        if (dx > 1 || dx < -1 || dy > 1 || dy < -1) xl = INF, xh = -INF;
-        ws.cnear[lane] = make_float4(xl, xh, yl, yh);
     }
     int incl = warp_incl_scan(cnt, lane);
     if (lane < nsrc) ws.cpre[lane + 1] = incl;
@@ -136,50 +138,91 @@ __device__ void setup_tables(const KParams &kp, const Item &it, WarpSmem &ws, in
 
 // Source record for stream index i (null record far away past the end), in
 // the pencil frame.  FLAG: w = 1 if the source may lie within eps of a sink
-// of the pencil (single spline), else 0.
+// of the tile (single spline), else 0: it must lie inside the tile's sink
+// bounding box widened by eps (x, y from ws.tbb; z in [zlo, zhi]; source
+// cells share the pencil's z cell, so z needs no shift).
 template <bool FLAG>
 __device__ __forceinline__ float4 load_src(const KParams &kp, const WarpSmem &ws, int i,
-                                           int src_end, int &k) {
+                                           int src_end, int &k, float zlo, float zhi) {
     if (i >= src_end) return make_float4(1e18f, 1e18f, 1e18f, 0.f);
     while (i >= ws.cpre[k + 1]) k++;
     int64_t p = ws.cstart[k] + (i - ws.cpre[k]);
     float4 t = __ldg(&kp.pos[p]);
-    if (FLAG) {
-        float4 nr = ws.cnear[k];
-        t.w = (t.x >= nr.x && t.x <= nr.y && t.y >= nr.z && t.y <= nr.w) ? 1.f : 0.f;
-    }
     t.x += ws.csx[k];
     t.y += ws.csy[k];
+    if (FLAG) {
+        const float4 bb = ws.tbb;
+        t.w = (t.x >= bb.x && t.x <= bb.y && t.y >= bb.z && t.y <= bb.w && t.z >= zlo &&
+               t.z <= zhi)
+                  ? 1.f
+                  : 0.f;
+    }
     return t;
 }
 
-// One staged chunk (m_pad sources, a multiple of UNR) against the lane's S
-// sinks, accumulated straight into the running partials.  NEAR selects the
-// both-branch single-spline evaluation (source cells adjacent to the sink cell).
-template <int SOFT, bool DENS, int S, bool NEAR, int UNR>
-__device__ __forceinline__ void chunk_pairs(const float4 *buf, int m_pad, const float (&sx)[S],
-                                            const float (&sy)[S], const float (&sz)[S],
-                                            float (&px)[S], float (&py)[S], float (&pz)[S],
-                                            float (&pw)[S], const PairConst &pc) {
+// One staged chunk (m_pad sources, a multiple of UNR) against the lane's
+// sinks, accumulated straight into the running partials.  Separations are
+// taken sink - source, so a += g * d.  NEAR selects the both-branch single
+// spline evaluation.  Scalar form: one sink per lane.
+template <int SOFT, bool DENS, bool NEAR, int UNR>
+__device__ __forceinline__ void chunk_scalar(const float4 *bxy, const float2 *bz, int m_pad,
+                                             float sx, float sy, float sz, float &px, float &py,
+                                             float &pz, float &pw, const PairConst &pc) {
 #pragma unroll 1
     for (int j = 0; j < m_pad; j += UNR) {
 #pragma unroll
         for (int u = 0; u < UNR; u++) {
-            float4 t = buf[j + u];
+            float4 t = bxy[j + u];
+            float tz = bz[j + u].x;
+            float dx = sx + t.x, dy = sy + t.z, dz = sz + tz;
+            float g;
+            if (NEAR) {
+                g = spline_g_both(dx, dy, dz, pc);
+            } else {
+                float r2;
+                g = pair_g_fast<SOFT>(dx, dy, dz, pc, r2);
+            }
+            px = fmaf(g, dx, px);
+            py = fmaf(g, dy, py);
+            pz = fmaf(g, dz, pz);
+            if (DENS) pw += dens_term(dx, dy, dz, pc.b2);
+        }
+    }
+}
+
+// Paired form: SP pairs of sinks per lane, two sinks per FP32 instruction.
+template <int SOFT, bool DENS, int SP, bool NEAR, int UNR>
+__device__ __forceinline__ void chunk_paired(const float4 *bxy, const float2 *bz, int m_pad,
+                                             const float2 (&sx)[SP], const float2 (&sy)[SP],
+                                             const float2 (&sz)[SP], float2 (&px)[SP],
+                                             float2 (&py)[SP], float2 (&pz)[SP],
+                                             float2 (&pw)[SP], const PairConst &pc) {
+#pragma unroll 1
+    for (int j = 0; j < m_pad; j += UNR) {
 #pragma unroll
-            for (int s = 0; s < S; s++) {
-                float dx = t.x - sx[s], dy = t.y - sy[s], dz = t.z - sz[s];
-                float g;
-                if (NEAR) {
-                    g = spline_g_both(dx, dy, dz, pc);
-                } else {
+        for (int u = 0; u < UNR; u++) {
+            float4 t = bxy[j + u];
+            float2 tz = bz[j + u];
+            float2 tx = make_float2(t.x, t.y), ty = make_float2(t.z, t.w);
+#pragma unroll
+            for (int q = 0; q < SP; q++) {
+                float2 dx = add2(sx[q], tx), dy = add2(sy[q], ty), dz = add2(sz[q], tz);
+                float2 g;
+                if (SOFT == SOFT_PLUMMER || SOFT == SOFT_SINGLE_SPLINE) {
+                    float2 r2 = r2_x2(dx, dy, dz, SOFT == SOFT_PLUMMER ? pc.eps : 1e-25f);
+                    g = NEAR ? spline_g_both_x2(r2, pc) : inv_r3_x2(r2);
+                } else {  // the cubic kernels: component-wise scalar evaluation
                     float r2;
-                    g = pair_g_fast<SOFT>(dx, dy, dz, pc, r2);
+                    g.x = pair_g_fast<SOFT>(dx.x, dy.x, dz.x, pc, r2);
+                    g.y = pair_g_fast<SOFT>(dx.y, dy.y, dz.y, pc, r2);
                 }
-                px[s] = fmaf(-g, dx, px[s]);
-                py[s] = fmaf(-g, dy, py[s]);
-                pz[s] = fmaf(-g, dz, pz[s]);
-                if (DENS) pw[s] += dens_term(dx, dy, dz, pc.b2);
+                px[q] = fma2(g, dx, px[q]);
+                py[q] = fma2(g, dy, py[q]);
+                pz[q] = fma2(g, dz, pz[q]);
+                if (DENS) {
+                    pw[q].x += dens_term(dx.x, dy.x, dz.x, pc.b2);
+                    pw[q].y += dens_term(dx.y, dy.y, dz.y, pc.b2);
+                }
             }
         }
     }
@@ -197,25 +240,24 @@ __device__ __forceinline__ int64_t sink_particle(const WarpSmem &ws, int i, int 
     return ws.sstart[a] + (i - ws.spre[a]);
 }
 
-template <int S>
-__device__ __forceinline__ void fold(float (&h)[S], float (&l)[S], float (&p)[S], bool plain) {
-#pragma unroll
-    for (int s = 0; s < S; s++) {
-        if (plain) {
-            h[s] += p[s];
-        } else {
-            float e;
-            two_sum(h[s], p[s], h[s], e);
-            l[s] += e;
-        }
-        p[s] = 0.f;
+// Fold one chunk partial p into the running (hi, lo) TwoSum pair (plain:
+// one FP32 running sum) and clear it.
+__device__ __forceinline__ void fold1(float &h, float &l, float &p, bool plain) {
+    if (plain) {
+        h += p;
+    } else {
+        float e;
+        two_sum(h, p, h, e);
+        l += e;
     }
+    p = 0.f;
 }
 
 template <int SOFT, bool DENS, int S, int UNR>
 __device__ void run_tile(const KParams &kp, WarpSmem &ws, const Item &it, int lane,
                          CombSmem *comb, int wslot) {
     const int NC = DENS ? 4 : 3;
+    constexpr int SP = S >= 2 ? S / 2 : 1;  // sink pairs of the paired form
     float sx[S], sy[S], sz[S];
 #pragma unroll
     for (int s = 0; s < S; s++) {
@@ -230,42 +272,117 @@ __device__ void run_tile(const KParams &kp, WarpSmem &ws, const Item &it, int la
             sz[s] = q.z + kp.zshift[a];
         }
     }
-    float hx[S], hy[S], hz[S], lx[S], ly[S], lz[S], px[S], py[S], pz[S], pw[S];
+    // running sums (hi, lo) per sink; chunk partials: scalar (S == 1) or
+    // pairs of sinks 2q, 2q+1
+    float hx[S], hy[S], hz[S], lx[S], ly[S], lz[S];
 #pragma unroll
-    for (int s = 0; s < S; s++)
-        hx[s] = hy[s] = hz[s] = lx[s] = ly[s] = lz[s] = px[s] = py[s] = pz[s] = pw[s] = 0.f;
+    for (int s = 0; s < S; s++) hx[s] = hy[s] = hz[s] = lx[s] = ly[s] = lz[s] = 0.f;
+    float px1 = 0.f, py1 = 0.f, pz1 = 0.f, pw1 = 0.f;
+    float2 qx[SP], qy[SP], qz[SP], px[SP], py[SP], pz[SP], pw[SP];
+#pragma unroll
+    for (int q = 0; q < SP; q++) {
+        if (S >= 2) {
+            qx[q] = make_float2(sx[2 * q], sx[2 * q + 1]);
+            qy[q] = make_float2(sy[2 * q], sy[2 * q + 1]);
+            qz[q] = make_float2(sz[2 * q], sz[2 * q + 1]);
+        }
+        px[q] = py[q] = pz[q] = pw[q] = make_float2(0.f, 0.f);
+    }
     constexpr bool FLAG = SOFT == SOFT_SINGLE_SPLINE;
     const bool plain = kp.plain;
+    // the tile's sink bounding box (pencil frame), widened by eps: sources
+    // outside it cannot be near any of the tile's sinks
+    float zlo = 3.0e38f, zhi = -3.0e38f;
+    if (FLAG) {
+        float xlo = 3.0e38f, xhi = -3.0e38f, ylo = 3.0e38f, yhi = -3.0e38f;
+#pragma unroll
+        for (int s = 0; s < S; s++)
+            if (s * 32 + lane < it.nsink) {
+                xlo = fminf(xlo, sx[s]);
+                xhi = fmaxf(xhi, sx[s]);
+                ylo = fminf(ylo, sy[s]);
+                yhi = fmaxf(yhi, sy[s]);
+                zlo = fminf(zlo, sz[s]);
+                zhi = fmaxf(zhi, sz[s]);
+            }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            xlo = fminf(xlo, __shfl_xor_sync(FULL, xlo, off));
+            xhi = fmaxf(xhi, __shfl_xor_sync(FULL, xhi, off));
+            ylo = fminf(ylo, __shfl_xor_sync(FULL, ylo, off));
+            yhi = fmaxf(yhi, __shfl_xor_sync(FULL, yhi, off));
+            zlo = fminf(zlo, __shfl_xor_sync(FULL, zlo, off));
+            zhi = fmaxf(zhi, __shfl_xor_sync(FULL, zhi, off));
+        }
+        const float w = kp.near_w;
+        __syncwarp();
+        if (lane == 0) ws.tbb = make_float4(xlo - w, xhi + w, ylo - w, yhi + w);
+        __syncwarp();
+        zlo -= w;
+        zhi += w;
+    }
     int k0 = 0, k1 = 0;
     int base = it.src_begin;
     // two sources per lane per chunk: stream indices base+lane, base+32+lane
-    float4 pre0 = load_src<FLAG>(kp, ws, base + lane, it.src_end, k0);
-    float4 pre1 = load_src<FLAG>(kp, ws, base + 32 + lane, it.src_end, k1);
+    float4 pre0 = load_src<FLAG>(kp, ws, base + lane, it.src_end, k0, zlo, zhi);
+    float4 pre1 = load_src<FLAG>(kp, ws, base + 32 + lane, it.src_end, k1, zlo, zhi);
     for (; base < it.src_end; base += CHUNK) {
-        // a chunk takes the both-branch path only if one of its sources may
-        // lie within eps of one of the tile's sinks
-        bool near = FLAG && __any_sync(FULL, pre0.w + pre1.w != 0.f);
+        // each half chunk (32 sources) takes the both-branch path only if
+        // one of its sources may lie within eps of one of the tile's sinks
+        bool near0 = FLAG && __any_sync(FULL, pre0.w != 0.f);
+        bool near1 = FLAG && __any_sync(FULL, pre1.w != 0.f);
         __syncwarp();
-        ws.buf[lane] = pre0;
-        ws.buf[lane + 32] = pre1;
+        ws.bxy[lane] = make_float4(-pre0.x, -pre0.x, -pre0.y, -pre0.y);
+        ws.bz[lane] = make_float2(-pre0.z, -pre0.z);
+        ws.bxy[lane + 32] = make_float4(-pre1.x, -pre1.x, -pre1.y, -pre1.y);
+        ws.bz[lane + 32] = make_float2(-pre1.z, -pre1.z);
         __syncwarp();
         if (base + CHUNK < it.src_end) {
-            pre0 = load_src<FLAG>(kp, ws, base + CHUNK + lane, it.src_end, k0);
-            pre1 = load_src<FLAG>(kp, ws, base + CHUNK + 32 + lane, it.src_end, k1);
+            pre0 = load_src<FLAG>(kp, ws, base + CHUNK + lane, it.src_end, k0, zlo, zhi);
+            pre1 = load_src<FLAG>(kp, ws, base + CHUNK + 32 + lane, it.src_end, k1, zlo, zhi);
         }
-        int m = min(CHUNK, it.src_end - base);
-        int m_pad = (m + UNR - 1) / UNR * UNR;
-        if constexpr (FLAG) {
-            if (near)
-                chunk_pairs<SOFT, DENS, S, true, UNR>(ws.buf, m_pad, sx, sy, sz, px, py, pz, pw, kp.pc);
-            else
-                chunk_pairs<SOFT, DENS, S, false, UNR>(ws.buf, m_pad, sx, sy, sz, px, py, pz, pw, kp.pc);
+        const int m = min(CHUNK, it.src_end - base);
+        const int halves = FLAG ? 2 : 1;  // the near decision is per half chunk
+#pragma unroll 1
+        for (int h = 0; h < halves; h++) {
+            const int mh = FLAG ? min(32, m - 32 * h) : m;
+            if (mh <= 0) break;
+            const int mpad = (mh + UNR - 1) / UNR * UNR;  // padding reads null records
+            const float4 *bxy = ws.bxy + 32 * h;
+            const float2 *bz = ws.bz + 32 * h;
+            const bool near = h ? near1 : near0;
+            if constexpr (S == 1) {
+                if (FLAG && near)
+                    chunk_scalar<SOFT, DENS, true, UNR>(bxy, bz, mpad, sx[0], sy[0], sz[0], px1, py1,
+                                                        pz1, pw1, kp.pc);
+                else
+                    chunk_scalar<SOFT, DENS, false, UNR>(bxy, bz, mpad, sx[0], sy[0], sz[0], px1,
+                                                         py1, pz1, pw1, kp.pc);
+            } else {
+                if (FLAG && near)
+                    chunk_paired<SOFT, DENS, SP, true, UNR>(bxy, bz, mpad, qx, qy, qz, px, py, pz, pw,
+                                                            kp.pc);
+                else
+                    chunk_paired<SOFT, DENS, SP, false, UNR>(bxy, bz, mpad, qx, qy, qz, px, py, pz,
+                                                             pw, kp.pc);
+            }
+        }
+        // fold every 64 sources
+        if constexpr (S == 1) {
+            fold1(hx[0], lx[0], px1, plain);
+            fold1(hy[0], ly[0], py1, plain);
+            fold1(hz[0], lz[0], pz1, plain);
         } else {
-            chunk_pairs<SOFT, DENS, S, false, UNR>(ws.buf, m_pad, sx, sy, sz, px, py, pz, pw, kp.pc);
+#pragma unroll
+            for (int q = 0; q < SP; q++) {
+                fold1(hx[2 * q], lx[2 * q], px[q].x, plain);
+                fold1(hx[2 * q + 1], lx[2 * q + 1], px[q].y, plain);
+                fold1(hy[2 * q], ly[2 * q], py[q].x, plain);
+                fold1(hy[2 * q + 1], ly[2 * q + 1], py[q].y, plain);
+                fold1(hz[2 * q], lz[2 * q], pz[q].x, plain);
+                fold1(hz[2 * q + 1], lz[2 * q + 1], pz[q].y, plain);
+            }
         }
-        fold<S>(hx, lx, px, plain);  // fold every 64 sources
-        fold<S>(hy, ly, py, plain);
-        fold<S>(hz, lz, pz, plain);
     }
 #pragma unroll
     for (int s = 0; s < S; s++) {
@@ -274,12 +391,14 @@ __device__ void run_tile(const KParams &kp, WarpSmem &ws, const Item &it, int la
         double vx = (double)hx[s] + (double)lx[s];
         double vy = (double)hy[s] + (double)ly[s];
         double vz = (double)hz[s] + (double)lz[s];
+        double vw = 0.0;
+        if (DENS) vw = S == 1 ? (double)pw1 : (double)((s & 1) ? pw[s >> 1].y : pw[s >> 1].x);
         if (comb) {  // split tiles hold at most TILE_MAX sinks (host-built)
             if (j >= TILE_MAX) continue;
             comb->v[wslot][0][j] = vx;
             comb->v[wslot][1][j] = vy;
             comb->v[wslot][2][j] = vz;
-            if (DENS) comb->v[wslot][3][j] = (double)pw[s];
+            if (DENS) comb->v[wslot][3][j] = vw;
         } else {
             int a;
             int64_t idx = sink_particle(ws, it.sink_begin + j, a) - kp.p0;
@@ -287,7 +406,7 @@ __device__ void run_tile(const KParams &kp, WarpSmem &ws, const Item &it, int la
             bp[0] = vx;
             bp[kp.n_range] = vy;
             bp[2 * kp.n_range] = vz;
-            if (DENS) bp[3 * kp.n_range] = (double)pw[s];
+            if (DENS) bp[3 * kp.n_range] = vw;
         }
     }
 }
@@ -357,18 +476,25 @@ __global__ void __launch_bounds__(WARPS_PER_CTA * 32, MINB) pencil_kernel(KParam
 
 // Sum the 2R+1 pencil partials of every particle in a fixed order, apply the
 // output scale (single spline: eps^3) and write accstruct records.
+// perm (optional): the caller's particle index of each packed slot; the
+// record of slot p0 + p goes to perm[p0 + p] - p0 (a permutation of the
+// range, since the in-cell ordering never moves a particle out of its cell).
 __global__ void coadd_kernel(const double *__restrict__ part, int64_t n, int W, int nc,
-                             double scale, int out_kind, void *out) {
+                             double scale, int out_kind, void *out,
+                             const uint32_t *__restrict__ perm, int64_t p0) {
     int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride) {
         double v[4] = {0.0, 0.0, 0.0, 0.0};
         for (int a = 0; a < W; a++)
-            for (int c = 0; c < nc; c++) v[c] += part[((int64_t)a * nc + c) * n + p];
+#pragma unroll
+            for (int c = 0; c < 4; c++)
+                if (c < nc) v[c] += part[((int64_t)a * nc + c) * n + p];
         float x = (float)(v[0] * scale), y = (float)(v[1] * scale), z = (float)(v[2] * scale);
+        const int64_t o_i = perm ? (int64_t)perm[p0 + p] - p0 : p;
         if (out_kind == NF_OUT_FLOAT4) {
-            reinterpret_cast<float4 *>(out)[p] = make_float4(x, y, z, nc == 4 ? (float)v[3] : 0.f);
+            reinterpret_cast<float4 *>(out)[o_i] = make_float4(x, y, z, nc == 4 ? (float)v[3] : 0.f);
         } else {
-            float *o = reinterpret_cast<float *>(out) + 3 * p;
+            float *o = reinterpret_cast<float *>(out) + 3 * o_i;
             o[0] = x;
             o[1] = y;
             o[2] = z;
@@ -381,6 +507,55 @@ __global__ void pack_positions(const float *__restrict__ x, const float *__restr
     int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride)
         out[p] = make_float4(x[p], y[p], z[p], 0.f);
+}
+
+// In-cell ordering of a resident box.  Particles keep their cell but are
+// ordered inside it along a Morton curve of their cell-relative position, so
+// that a tile of consecutive sinks covers a compact region: the tile's
+// bounding box then keeps most sources out of the single spline's
+// near-branch evaluation.  Key = cell id (high bits) : 30-bit Morton code.
+__device__ __forceinline__ uint32_t spread_bits10(uint32_t v) {
+    v &= 0x3ffu;
+    v = (v | (v << 16)) & 0x030000ffu;
+    v = (v | (v << 8)) & 0x0300f00fu;
+    v = (v | (v << 4)) & 0x030c30c3u;
+    v = (v | (v << 2)) & 0x09249249u;
+    return v;
+}
+
+__device__ __forceinline__ uint32_t cell_coord10(float u, int cpd) {
+    float t = fmaf(u, (float)cpd, 0.5f) * 1024.0f;  // cell-relative -> [0, 1024)
+    return (uint32_t)fminf(fmaxf(t, 0.0f), 1023.0f);
+}
+
+__global__ void order_keys(const float *__restrict__ x, const float *__restrict__ y,
+                           const float *__restrict__ z, const int64_t *__restrict__ cs,
+                           int64_t ncell, int cpd, int64_t n, uint64_t *key, uint32_t *val) {
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride) {
+        // cell of particle p: the last c with cs[c] <= p
+        int64_t lo = 0, hi = ncell;  // cs[lo] <= p < cs[hi]
+        while (hi - lo > 1) {
+            int64_t mid = (lo + hi) >> 1;
+            if (cs[mid] <= p) lo = mid;
+            else hi = mid;
+        }
+        uint32_t m = spread_bits10(cell_coord10(x[p], cpd)) << 2 |
+                     spread_bits10(cell_coord10(y[p], cpd)) << 1 |
+                     spread_bits10(cell_coord10(z[p], cpd));
+        key[p] = (uint64_t)lo << 30 | m;
+        val[p] = (uint32_t)p;
+    }
+}
+
+__global__ void pack_ordered(const float *__restrict__ x, const float *__restrict__ y,
+                             const float *__restrict__ z, const uint32_t *__restrict__ perm,
+                             int64_t n, float4 *out) {
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride) {
+        uint32_t q = perm[p];
+        out[p] = make_float4(x[q], y[q], z[q], 0.f);
+    }
 }
 
 // ------------------------------------------------------------------------
@@ -400,8 +575,8 @@ static const Variant VARIANTS[] = {
     {4, 8, 2, "sinks/lane<=4 unroll 8, 2 CTAs/SM"},
     {4, 4, 2, "sinks/lane<=4 unroll 4, 2 CTAs/SM"},
     {8, 4, 1, "sinks/lane<=8 unroll 4, 1 CTA/SM"},
-    {2, 8, 3, "sinks/lane<=2 unroll 8, 3 CTAs/SM"},
-    {2, 4, 4, "sinks/lane<=2 unroll 4, 4 CTAs/SM"},
+    {2, 4, 3, "sinks/lane<=2 unroll 4, 3 CTAs/SM"},
+    {2, 2, 4, "sinks/lane<=2 unroll 2, 4 CTAs/SM"},
 };
 static constexpr int NVARIANTS = sizeof(VARIANTS) / sizeof(VARIANTS[0]);
 
@@ -410,8 +585,8 @@ static KernelFn variant_kernel(int v) {
     switch (v) {
     case 1: return pencil_kernel<SOFT, DENS, 4, 4, 2>;
     case 2: return pencil_kernel<SOFT, DENS, 8, 4, 1>;
-    case 3: return pencil_kernel<SOFT, DENS, 2, 8, 3>;
-    case 4: return pencil_kernel<SOFT, DENS, 2, 4, 4>;
+    case 3: return pencil_kernel<SOFT, DENS, 2, 4, 3>;
+    case 4: return pencil_kernel<SOFT, DENS, 2, 2, 4>;
     default: return pencil_kernel<SOFT, DENS, 4, 8, 2>;
     }
 }
@@ -642,13 +817,10 @@ static KParams params_from(nf_ctx *ctx, const EngineLaunch &L) {
         kp.pc.c3 = (float)(10.0 * pow(ie2, 1.5));
     }
     {
-        // face slabs of width eps (+1% and a rounding allowance) on either
-        // side of the pencil column, in a source cell's own frame
+        // margin of the near test: eps (+1% and a rounding allowance)
         double h = 1.0 / (double)L.cpd;
         double e = cfg.softening == SOFT_SINGLE_SPLINE ? 1.0 / sqrt((double)eps) : 0.0;
-        double w = e * 1.01 + 1e-6 * h;
-        kp.face_lo = (float)(-0.5 * h + w);
-        kp.face_hi = (float)(0.5 * h - w);
+        kp.near_w = (float)(e * 1.01 + 1e-6 * h);
     }
     double h = 1.0 / (double)L.cpd;
     for (int a = 0; a < 2 * R + 1; a++) {
@@ -715,12 +887,12 @@ nf_status engine_launch(nf_ctx *ctx, const EngineLaunch &L, double, cudaStream_t
 }
 
 nf_status engine_coadd(nf_ctx *ctx, const double *part, int64_t n, void *out, cudaStream_t st,
-                       float eps) {
+                       float eps, const uint32_t *perm, int64_t p0) {
     if (n <= 0) return NF_OK;
     const nf_config &cfg = ctx->cfg;
     coadd_kernel<<<ctx->sms * 8, 256, 0, st>>>(part, n, 2 * cfg.near_field_radius + 1,
                                               cfg.b2 > 0.f ? 4 : 3, output_scale(cfg, eps),
-                                              cfg.out_kind, out);
+                                              cfg.out_kind, out, perm, p0);
     NF_CUDA(cudaGetLastError());
     return NF_OK;
 }
@@ -749,7 +921,7 @@ static nf_status enqueue_forces(nf_ctx *ctx, nf_box *box, Plan &pl, cudaStream_t
         int W = 2 * cfg.near_field_radius + 1;
         int blocks = ctx->sms * 8;
         coadd_kernel<<<blocks, 256, 0, st>>>(box->d_part, pl.n_range, W, kp.nc, output_scale(cfg, box->eps),
-                                            cfg.out_kind, pl.d_out);
+                                            cfg.out_kind, pl.d_out, box->d_perm, pl.p0);
         NF_CUDA(cudaGetLastError());
     }
     NF_CUDA(cudaEventRecordWithFlags(ctx->ev[2], st, cudaEventRecordExternal));
@@ -762,7 +934,8 @@ using namespace nf;
 
 size_t nf_box::device_bytes() const {
     size_t b = (size_t)np * sizeof(float4) + cell_start.size() * sizeof(int64_t) + part_bytes +
-               (d_stage ? 3 * (size_t)np * sizeof(float) : 0);
+               (d_stage ? 3 * (size_t)np * sizeof(float) : 0) + sort_bytes +
+               (d_perm ? (size_t)np * sizeof(uint32_t) : 0);
     for (auto &kv : plans) {
         b += kv.second->out_bytes + (size_t)kv.second->n_light * sizeof(Item) +
              (size_t)kv.second->n_heavy_groups * WARPS_PER_CTA * sizeof(Item);
@@ -779,6 +952,10 @@ extern "C" nf_status nf_box_create(nf_ctx *ctx, int cpd, int64_t np, const int64
     }
     if (cpd < 2 * ctx->cfg.near_field_radius + 1 || (cpd & 1) == 0 || np < 0) {
         set_error("nf_box_create: cpd must be odd and >= 2R+1");
+        return NF_EINVAL;
+    }
+    if (np >= ((int64_t)1 << 31) || (int64_t)cpd * cpd * cpd >= ((int64_t)1 << 34)) {
+        set_error("nf_box_create: at most 2^31 - 1 particles and 2^34 cells per box");
         return NF_EINVAL;
     }
     int64_t ncell = (int64_t)cpd * cpd * cpd;
@@ -833,17 +1010,60 @@ extern "C" nf_status nf_box_update(nf_ctx *ctx, nf_box *box, const float *x, con
             return NF_ENOMEM;
         }
     }
+    const int64_t n = box->np;
+    const int64_t ncell = (int64_t)box->cpd * box->cpd * box->cpd;
+    // in-cell ordering scratch: keys in/out, values in, radix-sort temp; the
+    // sorted values are the box's permutation
+    int key_bits = 30;
+    while (key_bits < 64 && ((uint64_t)1 << (key_bits - 30)) < (uint64_t)ncell) key_bits++;
+    size_t temp = 0;
+    cudaError_t e = cub::DeviceRadixSort::SortPairs(
+        nullptr, temp, (const uint64_t *)nullptr, (uint64_t *)nullptr, (const uint32_t *)nullptr,
+        (uint32_t *)nullptr, (int)n, 0, key_bits, ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "nf_box_update (ordering size query)");
+    const size_t kb = ((size_t)n * 8 + 255) & ~(size_t)255, vb = ((size_t)n * 4 + 255) & ~(size_t)255;
+    const size_t need = 2 * kb + vb + temp;
+    if (box->sort_bytes < need) {
+        cudaFree(box->d_sort);
+        box->d_sort = nullptr;
+        box->sort_bytes = 0;
+        if (cudaMalloc(&box->d_sort, need) != cudaSuccess) {
+            cudaGetLastError();
+            box->d_sort = nullptr;
+            set_error("nf_box_update: device allocation failed (ordering scratch)");
+            return NF_ENOMEM;
+        }
+        box->sort_bytes = need;
+    }
+    if (!box->d_perm && cudaMalloc(&box->d_perm, vb) != cudaSuccess) {
+        cudaGetLastError();
+        box->d_perm = nullptr;
+        set_error("nf_box_update: device allocation failed (permutation)");
+        return NF_ENOMEM;
+    }
+    unsigned char *sb = (unsigned char *)box->d_sort;
+    uint64_t *k_in = (uint64_t *)sb, *k_out = (uint64_t *)(sb + kb);
+    uint32_t *v_in = (uint32_t *)(sb + 2 * kb);
+    void *d_temp = sb + 2 * kb + vb;
     float *tmp = box->d_stage;
-    cudaError_t e = cudaMemcpyAsync(tmp, x, bytes, cudaMemcpyDefault, ctx->stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(tmp + box->np, y, bytes, cudaMemcpyDefault, ctx->stream);
-    if (e == cudaSuccess)
-        e = cudaMemcpyAsync(tmp + 2 * box->np, z, bytes, cudaMemcpyDefault, ctx->stream);
+    cudaStream_t st = ctx->stream;
+    e = cudaMemcpyAsync(tmp, x, bytes, cudaMemcpyDefault, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(tmp + n, y, bytes, cudaMemcpyDefault, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(tmp + 2 * n, z, bytes, cudaMemcpyDefault, st);
     if (e == cudaSuccess) {
-        pack_positions<<<ctx->sms * 8, 256, 0, ctx->stream>>>(tmp, tmp + box->np, tmp + 2 * box->np,
-                                                            box->np, box->d_pos);
+        order_keys<<<ctx->sms * 8, 256, 0, st>>>(tmp, tmp + n, tmp + 2 * n, box->d_cs, ncell,
+                                                 box->cpd, n, k_in, v_in);
         e = cudaGetLastError();
     }
-    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e == cudaSuccess)
+        e = cub::DeviceRadixSort::SortPairs(d_temp, temp, k_in, k_out, v_in, box->d_perm, (int)n, 0,
+                                            key_bits, st);
+    if (e == cudaSuccess) {
+        pack_ordered<<<ctx->sms * 8, 256, 0, st>>>(tmp, tmp + n, tmp + 2 * n, box->d_perm, n,
+                                                   box->d_pos);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return cuda_fail(e, "nf_box_update");
     return NF_OK;
 }
@@ -856,6 +1076,8 @@ extern "C" void nf_box_destroy(nf_ctx *ctx, nf_box *box) {
     cudaFree(box->d_cs);
     cudaFree(box->d_part);
     cudaFree(box->d_stage);
+    cudaFree(box->d_perm);
+    cudaFree(box->d_sort);
     delete box;
 }
 
@@ -1229,7 +1451,7 @@ extern "C" nf_status nf_forces_noalloc(const nf_config *cfg, int cpd, const void
     NF_CUDA(cudaLaunchKernel((const void *)fn, dim3(tmp.sms * std::max(per_sm, 1)),
                              dim3(WARPS_PER_CTA * 32), args, smem, st));
     coadd_kernel<<<tmp.sms * 8, 256, 0, st>>>(L.part, n, 2 * R + 1, kp.nc, output_scale(*cfg),
-                                              cfg->out_kind, out);
+                                              cfg->out_kind, out, nullptr, 0);
     NF_CUDA(cudaGetLastError());
     return NF_OK;
 }

@@ -74,8 +74,10 @@ struct EngineLaunch {
     float eps = 0.f;              // softening parameter (0: the context's)
 };
 nf_status engine_launch(nf_ctx *ctx, const EngineLaunch &L, double box_h, cudaStream_t st);
+// perm (optional): the caller's index of each packed slot; record p of the
+// range [p0, p0 + n) is written at perm[p0 + p] - p0.
 nf_status engine_coadd(nf_ctx *ctx, const double *part, int64_t n, void *out, cudaStream_t st,
-                       float eps = 0.f);
+                       float eps = 0.f, const uint32_t *perm = nullptr, int64_t p0 = 0);
 nf_status engine_pack(nf_ctx *ctx, const float *x, const float *y, const float *z, int64_t n,
                       float4 *out, cudaStream_t st);
 int engine_grid(nf_ctx *ctx, int variant);
@@ -101,6 +103,9 @@ struct nf_box {
     int64_t *d_cs = nullptr;          // cell_start on the device
     double *d_part = nullptr;         // pencil partials scratch
     float *d_stage = nullptr;         // position upload staging, 3 * np floats
+    uint32_t *d_perm = nullptr;       // caller's index of the particle in each packed slot
+    void *d_sort = nullptr;           // in-cell ordering scratch (keys, values, sort temp)
+    size_t sort_bytes = 0;
     size_t part_bytes = 0;
     std::map<std::pair<int, int>, std::unique_ptr<nf::Plan>> plans;
     int variant = -1;       // kernel shape chosen by the autotuner (-1: not tuned yet)

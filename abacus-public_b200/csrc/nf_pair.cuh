@@ -129,6 +129,46 @@ __device__ __forceinline__ float spline_g_both(float dx, float dy, float dz,
     return fminf(gfar, gnear);
 }
 
+// ---------------------------------------------------------------------------
+// Two sinks per instruction.  sm_100 executes FP32 add/mul/fma on register
+// pairs (f32x2): one issue slot for two results, the same per-component
+// rounding as the scalar instruction.  The pair loop is issue-bound in
+// scalar form (~15 issue slots per pair against 14 FP32 results), so pairing
+// the sinks of a lane moves the bound to the FP32 pipe itself.  Each helper
+// below is the component-wise twin of the scalar code above, operation for
+// operation, so a paired evaluation is bit-identical to the scalar one.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 dup2(float v) { return make_float2(v, v); }
+
+// inv_r3 on a pair.
+__device__ __forceinline__ float2 inv_r3_x2(float2 r2) {
+    float2 y = make_float2(rsqrt_est(r2.x), rsqrt_est(r2.y));
+    float2 y2 = mul2(y, y);
+    float2 y3 = mul2(y2, y);
+    float2 e = fma2(r2, y2, dup2(-1.0f));
+    float2 g = mul2(y3, e);
+    return fma2(g, dup2(-1.5f), y3);
+}
+
+// r^2 (+ the kernel's additive constant a2) of a pair of separations.
+__device__ __forceinline__ float2 r2_x2(float2 dx, float2 dy, float2 dz, float a2) {
+    return fma2(dz, dz, fma2(dy, dy, fma2(dx, dx, dup2(a2))));
+}
+
+// spline_g_both on a pair (r2 already floored by its 1e-25 addend).
+__device__ __forceinline__ float2 spline_g_both_x2(float2 r2, const PairConst &pc) {
+    float2 y = make_float2(rsqrt_est(r2.x), rsqrt_est(r2.y));
+    float2 y2 = mul2(y, y);
+    float2 e = fma2(r2, y2, dup2(-1.0f));
+    float2 yn = fma2(mul2(dup2(-0.5f), e), y, y);
+    float2 gfar = mul2(mul2(yn, yn), yn);
+    float2 gnear = fma2(fma2(dup2(pc.c1), yn, dup2(pc.c2)), r2, dup2(pc.c3));
+    return make_float2(fminf(gfar.x, gnear.x), fminf(gfar.y, gnear.y));
+}
+
 // Unsoftened r^2 for the FOF density sum (w += b2 - r^2 if r^2 < b2).
 __device__ __forceinline__ float dens_term(float dx, float dy, float dz, float b2) {
     float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));

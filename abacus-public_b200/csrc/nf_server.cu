@@ -248,7 +248,8 @@ static nf_status launch_request(nf_server *s, Req *r, Slot &sl, const Plan *pl) 
     L.grid = pl->grid;
     L.eps = r->box->eps;
     nf_status st = engine_launch(ctx, L, 0.0, sl.stream);
-    if (st == NF_OK) st = engine_coadd(ctx, sl.part, pl->n_range, sl.out, sl.stream, r->box->eps);
+    if (st == NF_OK) st = engine_coadd(ctx, sl.part, pl->n_range, sl.out, sl.stream, r->box->eps, r->box->d_perm,
+                                          pl->p0);
     if (st != NF_OK) return st;
     size_t bytes = (size_t)pl->n_range * rec_bytes(ctx);
     if (bytes)
