@@ -240,8 +240,9 @@ __device__ __forceinline__ int64_t sink_particle(const WarpSmem &ws, int i, int 
     return ws.sstart[a] + (i - ws.spre[a]);
 }
 
-// Fold one chunk partial p into the running (hi, lo) TwoSum pair (plain:
-// one FP32 running sum) and clear it.
+// Fold a partial p into the running (hi, lo) TwoSum pair (plain: one FP32
+// running sum) and clear it.  Scalar and paired (two sinks) forms; a - b is
+// formed as fma(b, -1, a), which rounds exactly like a subtraction.
 __device__ __forceinline__ void fold1(float &h, float &l, float &p, bool plain) {
     if (plain) {
         h += p;
@@ -252,6 +253,24 @@ __device__ __forceinline__ void fold1(float &h, float &l, float &p, bool plain) 
     }
     p = 0.f;
 }
+
+__device__ __forceinline__ void fold2(float2 &h, float2 &l, float2 &p, bool plain) {
+    if (plain) {
+        h = add2(h, p);
+    } else {
+        const float2 m1 = dup2(-1.0f);
+        float2 s = add2(h, p);
+        float2 bb = fma2(h, m1, s);                  // s - h
+        float2 ea = fma2(fma2(bb, m1, s), m1, h);    // h - (s - bb)
+        float2 eb = fma2(bb, m1, p);                 // p - bb
+        l = add2(l, add2(ea, eb));
+        h = s;
+    }
+    p = make_float2(0.f, 0.f);
+}
+
+// FP32 partials are folded into the (hi, lo) pairs every FOLD_CHUNKS chunks.
+constexpr int FOLD_CHUNKS = 2;
 
 template <int SOFT, bool DENS, int S, int UNR>
 __device__ void run_tile(const KParams &kp, WarpSmem &ws, const Item &it, int lane,
@@ -272,13 +291,12 @@ __device__ void run_tile(const KParams &kp, WarpSmem &ws, const Item &it, int la
             sz[s] = q.z + kp.zshift[a];
         }
     }
-    // running sums (hi, lo) per sink; chunk partials: scalar (S == 1) or
-    // pairs of sinks 2q, 2q+1
-    float hx[S], hy[S], hz[S], lx[S], ly[S], lz[S];
-#pragma unroll
-    for (int s = 0; s < S; s++) hx[s] = hy[s] = hz[s] = lx[s] = ly[s] = lz[s] = 0.f;
+    // scalar form (S == 1): partial p*1 and running (h*1, l*1); paired form:
+    // sinks 2q, 2q+1 in the two halves of qx/qy/qz, px.., hx.., lx..
     float px1 = 0.f, py1 = 0.f, pz1 = 0.f, pw1 = 0.f;
+    float hx1 = 0.f, hy1 = 0.f, hz1 = 0.f, lx1 = 0.f, ly1 = 0.f, lz1 = 0.f;
     float2 qx[SP], qy[SP], qz[SP], px[SP], py[SP], pz[SP], pw[SP];
+    float2 hx[SP], hy[SP], hz[SP], lx[SP], ly[SP], lz[SP];
 #pragma unroll
     for (int q = 0; q < SP; q++) {
         if (S >= 2) {
@@ -287,6 +305,7 @@ __device__ void run_tile(const KParams &kp, WarpSmem &ws, const Item &it, int la
             qz[q] = make_float2(sz[2 * q], sz[2 * q + 1]);
         }
         px[q] = py[q] = pz[q] = pw[q] = make_float2(0.f, 0.f);
+        hx[q] = hy[q] = hz[q] = lx[q] = ly[q] = lz[q] = make_float2(0.f, 0.f);
     }
     constexpr bool FLAG = SOFT == SOFT_SINGLE_SPLINE;
     const bool plain = kp.plain;
@@ -326,61 +345,50 @@ __device__ void run_tile(const KParams &kp, WarpSmem &ws, const Item &it, int la
     // two sources per lane per chunk: stream indices base+lane, base+32+lane
     float4 pre0 = load_src<FLAG>(kp, ws, base + lane, it.src_end, k0, zlo, zhi);
     float4 pre1 = load_src<FLAG>(kp, ws, base + 32 + lane, it.src_end, k1, zlo, zhi);
-    for (; base < it.src_end; base += CHUNK) {
-        // each half chunk (32 sources) takes the both-branch path only if
-        // one of its sources may lie within eps of one of the tile's sinks
-        bool near0 = FLAG && __any_sync(FULL, pre0.w != 0.f);
-        bool near1 = FLAG && __any_sync(FULL, pre1.w != 0.f);
+    for (int chunk = 1; base < it.src_end; base += CHUNK, chunk++) {
+        // the chunk takes the both-branch path only if one of its sources
+        // may lie within eps of one of the tile's sinks
+        const bool near = FLAG && __any_sync(FULL, pre0.w + pre1.w != 0.f);
         __syncwarp();
         ws.bxy[lane] = make_float4(-pre0.x, -pre0.x, -pre0.y, -pre0.y);
         ws.bz[lane] = make_float2(-pre0.z, -pre0.z);
         ws.bxy[lane + 32] = make_float4(-pre1.x, -pre1.x, -pre1.y, -pre1.y);
         ws.bz[lane + 32] = make_float2(-pre1.z, -pre1.z);
         __syncwarp();
-        if (base + CHUNK < it.src_end) {
+        const bool more = base + CHUNK < it.src_end;
+        if (more) {
             pre0 = load_src<FLAG>(kp, ws, base + CHUNK + lane, it.src_end, k0, zlo, zhi);
             pre1 = load_src<FLAG>(kp, ws, base + CHUNK + 32 + lane, it.src_end, k1, zlo, zhi);
         }
         const int m = min(CHUNK, it.src_end - base);
-        const int halves = FLAG ? 2 : 1;  // the near decision is per half chunk
-#pragma unroll 1
-        for (int h = 0; h < halves; h++) {
-            const int mh = FLAG ? min(32, m - 32 * h) : m;
-            if (mh <= 0) break;
-            const int mpad = (mh + UNR - 1) / UNR * UNR;  // padding reads null records
-            const float4 *bxy = ws.bxy + 32 * h;
-            const float2 *bz = ws.bz + 32 * h;
-            const bool near = h ? near1 : near0;
-            if constexpr (S == 1) {
-                if (FLAG && near)
-                    chunk_scalar<SOFT, DENS, true, UNR>(bxy, bz, mpad, sx[0], sy[0], sz[0], px1, py1,
-                                                        pz1, pw1, kp.pc);
-                else
-                    chunk_scalar<SOFT, DENS, false, UNR>(bxy, bz, mpad, sx[0], sy[0], sz[0], px1,
-                                                         py1, pz1, pw1, kp.pc);
-            } else {
-                if (FLAG && near)
-                    chunk_paired<SOFT, DENS, SP, true, UNR>(bxy, bz, mpad, qx, qy, qz, px, py, pz, pw,
-                                                            kp.pc);
-                else
-                    chunk_paired<SOFT, DENS, SP, false, UNR>(bxy, bz, mpad, qx, qy, qz, px, py, pz,
-                                                             pw, kp.pc);
-            }
-        }
-        // fold every 64 sources
+        const int mpad = (m + UNR - 1) / UNR * UNR;  // padding reads null records
         if constexpr (S == 1) {
-            fold1(hx[0], lx[0], px1, plain);
-            fold1(hy[0], ly[0], py1, plain);
-            fold1(hz[0], lz[0], pz1, plain);
+            if (FLAG && near)
+                chunk_scalar<SOFT, DENS, true, UNR>(ws.bxy, ws.bz, mpad, sx[0], sy[0], sz[0], px1,
+                                                    py1, pz1, pw1, kp.pc);
+            else
+                chunk_scalar<SOFT, DENS, false, UNR>(ws.bxy, ws.bz, mpad, sx[0], sy[0], sz[0], px1,
+                                                     py1, pz1, pw1, kp.pc);
         } else {
+            if (FLAG && near)
+                chunk_paired<SOFT, DENS, SP, true, UNR>(ws.bxy, ws.bz, mpad, qx, qy, qz, px, py, pz,
+                                                        pw, kp.pc);
+            else
+                chunk_paired<SOFT, DENS, SP, false, UNR>(ws.bxy, ws.bz, mpad, qx, qy, qz, px, py, pz,
+                                                         pw, kp.pc);
+        }
+        if (chunk % FOLD_CHUNKS == 0 || !more) {
+            if constexpr (S == 1) {
+                fold1(hx1, lx1, px1, plain);
+                fold1(hy1, ly1, py1, plain);
+                fold1(hz1, lz1, pz1, plain);
+            } else {
 #pragma unroll
-            for (int q = 0; q < SP; q++) {
-                fold1(hx[2 * q], lx[2 * q], px[q].x, plain);
-                fold1(hx[2 * q + 1], lx[2 * q + 1], px[q].y, plain);
-                fold1(hy[2 * q], ly[2 * q], py[q].x, plain);
-                fold1(hy[2 * q + 1], ly[2 * q + 1], py[q].y, plain);
-                fold1(hz[2 * q], lz[2 * q], pz[q].x, plain);
-                fold1(hz[2 * q + 1], lz[2 * q + 1], pz[q].y, plain);
+                for (int q = 0; q < SP; q++) {
+                    fold2(hx[q], lx[q], px[q], plain);
+                    fold2(hy[q], ly[q], py[q], plain);
+                    fold2(hz[q], lz[q], pz[q], plain);
+                }
             }
         }
     }
@@ -388,11 +396,20 @@ __device__ void run_tile(const KParams &kp, WarpSmem &ws, const Item &it, int la
     for (int s = 0; s < S; s++) {
         int j = s * 32 + lane;
         if (j >= it.nsink) continue;
-        double vx = (double)hx[s] + (double)lx[s];
-        double vy = (double)hy[s] + (double)ly[s];
-        double vz = (double)hz[s] + (double)lz[s];
-        double vw = 0.0;
-        if (DENS) vw = S == 1 ? (double)pw1 : (double)((s & 1) ? pw[s >> 1].y : pw[s >> 1].x);
+        double vx, vy, vz, vw = 0.0;
+        if constexpr (S == 1) {
+            vx = (double)hx1 + (double)lx1;
+            vy = (double)hy1 + (double)ly1;
+            vz = (double)hz1 + (double)lz1;
+            if (DENS) vw = (double)pw1;
+        } else {
+            const int q = s >> 1;
+            const bool odd = s & 1;
+            vx = (double)(odd ? hx[q].y : hx[q].x) + (double)(odd ? lx[q].y : lx[q].x);
+            vy = (double)(odd ? hy[q].y : hy[q].x) + (double)(odd ? ly[q].y : ly[q].x);
+            vz = (double)(odd ? hz[q].y : hz[q].x) + (double)(odd ? lz[q].y : lz[q].x);
+            if (DENS) vw = (double)(odd ? pw[q].y : pw[q].x);
+        }
         if (comb) {  // split tiles hold at most TILE_MAX sinks (host-built)
             if (j >= TILE_MAX) continue;
             comb->v[wslot][0][j] = vx;
@@ -573,7 +590,7 @@ struct Variant {
 };
 static const Variant VARIANTS[] = {
     {4, 8, 2, "sinks/lane<=4 unroll 8, 2 CTAs/SM"},
-    {4, 4, 2, "sinks/lane<=4 unroll 4, 2 CTAs/SM"},
+    {4, 16, 2, "sinks/lane<=4 unroll 16, 2 CTAs/SM"},
     {8, 4, 1, "sinks/lane<=8 unroll 4, 1 CTA/SM"},
     {2, 4, 3, "sinks/lane<=2 unroll 4, 3 CTAs/SM"},
     {2, 2, 4, "sinks/lane<=2 unroll 2, 4 CTAs/SM"},
@@ -583,7 +600,7 @@ static constexpr int NVARIANTS = sizeof(VARIANTS) / sizeof(VARIANTS[0]);
 template <int SOFT, bool DENS>
 static KernelFn variant_kernel(int v) {
     switch (v) {
-    case 1: return pencil_kernel<SOFT, DENS, 4, 4, 2>;
+    case 1: return pencil_kernel<SOFT, DENS, 4, 16, 2>;
     case 2: return pencil_kernel<SOFT, DENS, 8, 4, 1>;
     case 3: return pencil_kernel<SOFT, DENS, 2, 4, 3>;
     case 4: return pencil_kernel<SOFT, DENS, 2, 2, 4>;
