@@ -325,6 +325,11 @@ class DeviceBox:
     def update(self, x, y, z):
         check(lib().nf_box_update(self.ctx.h, self.h, _ptr(x), _ptr(y), _ptr(z)), "nf_box_update")
 
+    def update_device(self, x_ptr: int, y_ptr: int, z_ptr: int):
+        """New positions from device arrays (same cell counts)."""
+        check(lib().nf_box_update(self.ctx.h, self.h, ctypes.c_void_p(x_ptr), ctypes.c_void_p(y_ptr),
+                                  ctypes.c_void_p(z_ptr)), "nf_box_update")
+
     def slab_particles(self, lo: int, hi: int) -> tuple[int, int]:
         c2 = self.cpd * self.cpd
         return int(self._cs[lo * c2]), int(self._cs[hi * c2])
