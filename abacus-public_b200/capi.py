@@ -141,8 +141,17 @@ class RequestInfo(ctypes.Structure):
                 ("run_ms", ctypes.c_double), ("total_ms", ctypes.c_double)]
 
 
+class KickParams(ctypes.Structure):
+    _fields_ = [("near_scale", ctypes.c_float), ("rescale", ctypes.c_float),
+                ("kick1", ctypes.c_float), ("kick2", ctypes.c_float), ("b2", ctypes.c_float)]
+
+
 # Every symbol the header declares; the loader checks each one is exported.
 EXPORTS = {
+    "nf_box_update_aos": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "nf_box_kick": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                   ctypes.POINTER(KickParams), ctypes.c_void_p, ctypes.c_void_p,
+                                   ctypes.c_void_p, ctypes.c_void_p]),
     "nf_server_request_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64,
                                               ctypes.POINTER(RequestInfo)]),
     "nf_server_start": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ServerConfig),
@@ -324,6 +333,22 @@ class DeviceBox:
 
     def update(self, x, y, z):
         check(lib().nf_box_update(self.ctx.h, self.h, _ptr(x), _ptr(y), _ptr(z)), "nf_box_update")
+
+    def update_aos(self, xyz):
+        """New positions as (N, 3) float32 records (host array or device pointer)."""
+        ptr = ctypes.c_void_p(xyz) if isinstance(xyz, int) else _ptr(np.ascontiguousarray(xyz))
+        check(lib().nf_box_update_aos(self.ctx.h, self.h, ptr), "nf_box_update_aos")
+
+    def kick(self, lo: int, hi: int, vel_ptr: int, far_ptr: int = 0, acc_ptr: int = 0,
+             stats_ptr: int = 0, near_scale: float = 1.0, rescale: float = 1.0,
+             kick1: float = 0.0, kick2: float = 0.0, b2: float = 0.0):
+        """Near field of slabs [lo, hi) fused with the rescale/co-add with the far
+        field and the two half kicks (device pointers; see nf_box_kick)."""
+        k = KickParams(near_scale, rescale, kick1, kick2, b2)
+        check(lib().nf_box_kick(self.ctx.h, self.h, lo, hi, ctypes.byref(k),
+                                ctypes.c_void_p(far_ptr or None), ctypes.c_void_p(vel_ptr),
+                                ctypes.c_void_p(acc_ptr or None), ctypes.c_void_p(stats_ptr or None)),
+              "nf_box_kick")
 
     def update_device(self, x_ptr: int, y_ptr: int, z_ptr: int):
         """New positions from device arrays (same cell counts)."""

@@ -545,9 +545,12 @@ __device__ __forceinline__ uint32_t cell_coord10(float u, int cpd) {
     return (uint32_t)fminf(fmaxf(t, 0.0f), 1023.0f);
 }
 
+// Component c of particle p is at x/y/z[p * comp_stride] (1: three
+// arrays; 3: one array of (x, y, z) records).
 __global__ void order_keys(const float *__restrict__ x, const float *__restrict__ y,
-                           const float *__restrict__ z, const int64_t *__restrict__ cs,
-                           int64_t ncell, int cpd, int64_t n, uint64_t *key, uint32_t *val) {
+                           const float *__restrict__ z, int comp_stride,
+                           const int64_t *__restrict__ cs, int64_t ncell, int cpd, int64_t n,
+                           uint64_t *key, uint32_t *val) {
     int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride) {
         // cell of particle p: the last c with cs[c] <= p
@@ -557,21 +560,100 @@ __global__ void order_keys(const float *__restrict__ x, const float *__restrict_
             if (cs[mid] <= p) lo = mid;
             else hi = mid;
         }
-        uint32_t m = spread_bits10(cell_coord10(x[p], cpd)) << 2 |
-                     spread_bits10(cell_coord10(y[p], cpd)) << 1 |
-                     spread_bits10(cell_coord10(z[p], cpd));
+        const int64_t q = p * comp_stride;
+        uint32_t m = spread_bits10(cell_coord10(x[q], cpd)) << 2 |
+                     spread_bits10(cell_coord10(y[q], cpd)) << 1 |
+                     spread_bits10(cell_coord10(z[q], cpd));
         key[p] = (uint64_t)lo << 30 | m;
         val[p] = (uint32_t)p;
     }
 }
 
 __global__ void pack_ordered(const float *__restrict__ x, const float *__restrict__ y,
-                             const float *__restrict__ z, const uint32_t *__restrict__ perm,
-                             int64_t n, float4 *out) {
+                             const float *__restrict__ z, int comp_stride,
+                             const uint32_t *__restrict__ perm, int64_t n, float4 *out) {
     int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride) {
-        uint32_t q = perm[p];
+        int64_t q = (int64_t)perm[p] * comp_stride;
         out[p] = make_float4(x[q], y[q], z[q], 0.f);
+    }
+}
+
+// The step after the near field, fused with the co-add: the reference's
+// RescaleAndCoAddAcceleration (singlestep/Timestep/kick.cpp:72-107)
+//   a = (nacc * near_scale + facc) * rescale,  w = nacc.w - b2
+// and KickCell (kick.cpp:30-56)
+//   v += a kick1; cell stats of v and a; v += a kick2.
+// One warp per cell of the range; each particle's near acceleration is
+// co-added from its pencil partials exactly as coadd_kernel does (nacc is
+// the float record nf_box_forces would return), then the float operations
+// above run unfused, in the reference's order.  Cell stats: mean square
+// velocity (after the first half kick), max |v| and max |a| component.
+struct KickConst {
+    float near_scale, rescale, kick1, kick2, b2;
+};
+
+__global__ void kick_kernel(const double *__restrict__ part, int64_t n, int W, int nc,
+                            double scale, const int64_t *__restrict__ cs, int64_t c0,
+                            int64_t ncells, int64_t p0, const uint32_t *__restrict__ perm,
+                            KickConst k, const float *__restrict__ far, float *vel, void *acc_out,
+                            int out_kind, float *stats) {
+    const int lane = threadIdx.x & 31;
+    const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t c = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); c < ncells;
+         c += nwarps) {
+        const int64_t s0 = cs[c0 + c], s1 = cs[c0 + c + 1];
+        float sv2 = 0.f, mv = 0.f, ma = 0.f;
+        for (int64_t slot = s0 + lane; slot < s1; slot += 32) {
+            const int64_t i = slot - p0;
+            double v[4] = {0.0, 0.0, 0.0, 0.0};
+            for (int a = 0; a < W; a++)
+#pragma unroll
+                for (int q = 0; q < 4; q++)
+                    if (q < nc) v[q] += part[((int64_t)a * nc + q) * n + i];
+            const float nx = (float)(v[0] * scale), ny = (float)(v[1] * scale),
+                        nz = (float)(v[2] * scale), nw = nc == 4 ? (float)v[3] : 0.f;
+            const int64_t o = perm ? (int64_t)perm[slot] - p0 : i;
+            const float fx = far ? far[3 * o] : 0.f, fy = far ? far[3 * o + 1] : 0.f,
+                        fz = far ? far[3 * o + 2] : 0.f;
+            const float ax = __fmul_rn(__fadd_rn(__fmul_rn(nx, k.near_scale), fx), k.rescale);
+            const float ay = __fmul_rn(__fadd_rn(__fmul_rn(ny, k.near_scale), fy), k.rescale);
+            const float az = __fmul_rn(__fadd_rn(__fmul_rn(nz, k.near_scale), fz), k.rescale);
+            const float aw = __fsub_rn(nw, k.b2);
+            float vx = vel[3 * o], vy = vel[3 * o + 1], vz = vel[3 * o + 2];
+            vx = __fadd_rn(vx, __fmul_rn(ax, k.kick1));
+            vy = __fadd_rn(vy, __fmul_rn(ay, k.kick1));
+            vz = __fadd_rn(vz, __fmul_rn(az, k.kick1));
+            sv2 = __fadd_rn(sv2, __fadd_rn(__fadd_rn(__fmul_rn(vx, vx), __fmul_rn(vy, vy)),
+                                           __fmul_rn(vz, vz)));
+            mv = fmaxf(mv, fmaxf(fabsf(vx), fmaxf(fabsf(vy), fabsf(vz))));
+            ma = fmaxf(ma, fmaxf(fabsf(ax), fmaxf(fabsf(ay), fabsf(az))));
+            vel[3 * o] = __fadd_rn(vx, __fmul_rn(ax, k.kick2));
+            vel[3 * o + 1] = __fadd_rn(vy, __fmul_rn(ay, k.kick2));
+            vel[3 * o + 2] = __fadd_rn(vz, __fmul_rn(az, k.kick2));
+            if (acc_out) {
+                if (out_kind == NF_OUT_FLOAT4) {
+                    reinterpret_cast<float4 *>(acc_out)[o] = make_float4(ax, ay, az, aw);
+                } else {
+                    float *r = reinterpret_cast<float *>(acc_out) + 3 * o;
+                    r[0] = ax;
+                    r[1] = ay;
+                    r[2] = az;
+                }
+            }
+        }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            sv2 += __shfl_xor_sync(FULL, sv2, off);
+            mv = fmaxf(mv, __shfl_xor_sync(FULL, mv, off));
+            ma = fmaxf(ma, __shfl_xor_sync(FULL, ma, off));
+        }
+        if (lane == 0 && stats) {
+            const int64_t cnt = s1 - s0;
+            stats[3 * c] = cnt > 0 ? sv2 / (float)cnt : 0.f;
+            stats[3 * c + 1] = mv;
+            stats[3 * c + 2] = ma;
+        }
     }
 }
 
@@ -922,22 +1004,32 @@ nf_status engine_pack(nf_ctx *ctx, const float *x, const float *y, const float *
     return NF_OK;
 }
 
-static nf_status enqueue_forces(nf_ctx *ctx, nf_box *box, Plan &pl, cudaStream_t st) {
+// The pencil kernel of a plan into the box's partials, between events 0 and 1.
+static nf_status enqueue_pencil(nf_ctx *ctx, nf_box *box, Plan &pl, cudaStream_t st,
+                                unsigned evflags) {
     const nf_config &cfg = ctx->cfg;
     KParams kp = make_params(ctx, box, pl);
     KernelFn fn = pick_kernel(cfg.softening, cfg.b2 > 0.f, pl.variant);
     NF_CUDA(cudaMemsetAsync(pl.d_counters, 0, 2 * sizeof(int), st));
-    NF_CUDA(cudaEventRecordWithFlags(ctx->ev[0], st, cudaEventRecordExternal));
+    NF_CUDA(cudaEventRecordWithFlags(ctx->ev[0], st, evflags));
     if (pl.n_heavy_groups + pl.n_light > 0) {
         void *args[] = {&kp};
         NF_CUDA(cudaLaunchKernel((const void *)fn, dim3(pl.grid), dim3(WARPS_PER_CTA * 32), args,
                                  kernel_smem(), st));
     }
-    NF_CUDA(cudaEventRecordWithFlags(ctx->ev[1], st, cudaEventRecordExternal));
+    NF_CUDA(cudaEventRecordWithFlags(ctx->ev[1], st, evflags));
+    return NF_OK;
+}
+
+static nf_status enqueue_forces(nf_ctx *ctx, nf_box *box, Plan &pl, cudaStream_t st) {
+    const nf_config &cfg = ctx->cfg;
+    nf_status est = enqueue_pencil(ctx, box, pl, st, cudaEventRecordExternal);
+    if (est != NF_OK) return est;
+    const int nc = cfg.b2 > 0.f ? 4 : 3;
     if (pl.n_range > 0) {
         int W = 2 * cfg.near_field_radius + 1;
         int blocks = ctx->sms * 8;
-        coadd_kernel<<<blocks, 256, 0, st>>>(box->d_part, pl.n_range, W, kp.nc, output_scale(cfg, box->eps),
+        coadd_kernel<<<blocks, 256, 0, st>>>(box->d_part, pl.n_range, W, nc, output_scale(cfg, box->eps),
                                             cfg.out_kind, pl.d_out, box->d_perm, pl.p0);
         NF_CUDA(cudaGetLastError());
     }
@@ -1009,6 +1101,14 @@ extern "C" nf_status nf_box_create(nf_ctx *ctx, int cpd, int64_t np, const int64
     return st;
 }
 
+namespace nf {
+// Upload positions into a box: SoA (x, y, z arrays; aos == nullptr) or AoS
+// (aos = n records of three floats), host or device memory; then order the
+// particles inside their cells and pack them (ctx->mu held by the caller).
+static nf_status box_upload(nf_ctx *ctx, nf_box *box, const float *x, const float *y,
+                            const float *z, const float *aos);
+}  // namespace nf
+
 extern "C" nf_status nf_box_update(nf_ctx *ctx, nf_box *box, const float *x, const float *y,
                                    const float *z) {
     if (!ctx || !box || !x || !y || !z) {
@@ -1016,6 +1116,20 @@ extern "C" nf_status nf_box_update(nf_ctx *ctx, nf_box *box, const float *x, con
         return NF_EINVAL;
     }
     std::lock_guard<std::mutex> lk(ctx->mu);
+    return box_upload(ctx, box, x, y, z, nullptr);
+}
+
+extern "C" nf_status nf_box_update_aos(nf_ctx *ctx, nf_box *box, const float *xyz) {
+    if (!ctx || !box || (!xyz && box->np > 0)) {
+        set_error("nf_box_update_aos: null argument");
+        return NF_EINVAL;
+    }
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    return box_upload(ctx, box, nullptr, nullptr, nullptr, xyz);
+}
+
+static nf_status nf::box_upload(nf_ctx *ctx, nf_box *box, const float *x, const float *y,
+                                const float *z, const float *aos) {
     NF_CUDA(cudaSetDevice(ctx->device));
     // stage the three components through the box's device staging buffer
     size_t bytes = (size_t)box->np * sizeof(float);
@@ -1037,7 +1151,7 @@ extern "C" nf_status nf_box_update(nf_ctx *ctx, nf_box *box, const float *x, con
     cudaError_t e = cub::DeviceRadixSort::SortPairs(
         nullptr, temp, (const uint64_t *)nullptr, (uint64_t *)nullptr, (const uint32_t *)nullptr,
         (uint32_t *)nullptr, (int)n, 0, key_bits, ctx->stream);
-    if (e != cudaSuccess) return cuda_fail(e, "nf_box_update (ordering size query)");
+    if (e != cudaSuccess) return cuda_fail(e, "box upload (ordering size query)");
     const size_t kb = ((size_t)n * 8 + 255) & ~(size_t)255, vb = ((size_t)n * 4 + 255) & ~(size_t)255;
     const size_t need = 2 * kb + vb + temp;
     if (box->sort_bytes < need) {
@@ -1064,20 +1178,27 @@ extern "C" nf_status nf_box_update(nf_ctx *ctx, nf_box *box, const float *x, con
     void *d_temp = sb + 2 * kb + vb;
     float *tmp = box->d_stage;
     cudaStream_t st = ctx->stream;
-    e = cudaMemcpyAsync(tmp, x, bytes, cudaMemcpyDefault, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(tmp + n, y, bytes, cudaMemcpyDefault, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(tmp + 2 * n, z, bytes, cudaMemcpyDefault, st);
+    // staged components: SoA at tmp, tmp + n, tmp + 2n (stride 1) or the
+    // AoS records as given at tmp, tmp + 1, tmp + 2 (stride 3)
+    const float *sx = tmp, *sy = aos ? tmp + 1 : tmp + n, *sz = aos ? tmp + 2 : tmp + 2 * n;
+    const int cstride = aos ? 3 : 1;
+    if (aos) {
+        e = cudaMemcpyAsync(tmp, aos, 3 * bytes, cudaMemcpyDefault, st);
+    } else {
+        e = cudaMemcpyAsync(tmp, x, bytes, cudaMemcpyDefault, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(tmp + n, y, bytes, cudaMemcpyDefault, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(tmp + 2 * n, z, bytes, cudaMemcpyDefault, st);
+    }
     if (e == cudaSuccess) {
-        order_keys<<<ctx->sms * 8, 256, 0, st>>>(tmp, tmp + n, tmp + 2 * n, box->d_cs, ncell,
-                                                 box->cpd, n, k_in, v_in);
+        order_keys<<<ctx->sms * 8, 256, 0, st>>>(sx, sy, sz, cstride, box->d_cs, ncell, box->cpd, n,
+                                                 k_in, v_in);
         e = cudaGetLastError();
     }
     if (e == cudaSuccess)
         e = cub::DeviceRadixSort::SortPairs(d_temp, temp, k_in, k_out, v_in, box->d_perm, (int)n, 0,
                                             key_bits, st);
     if (e == cudaSuccess) {
-        pack_ordered<<<ctx->sms * 8, 256, 0, st>>>(tmp, tmp + n, tmp + 2 * n, box->d_perm, n,
-                                                   box->d_pos);
+        pack_ordered<<<ctx->sms * 8, 256, 0, st>>>(sx, sy, sz, cstride, box->d_perm, n, box->d_pos);
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
@@ -1321,6 +1442,49 @@ extern "C" nf_status nf_box_forces(nf_ctx *ctx, nf_box *box, int lo, int hi, voi
     ctx->last.pairs = pl->pairs;
     ctx->last.padded_pairs = pl->padded_pairs;
     ctx->last.launches = (pl->n_heavy_groups + pl->n_light > 0 ? 1 : 0) + (pl->n_range > 0 ? 1 : 0);
+    ctx->last.items = pl->n_heavy_groups * WARPS_PER_CTA + pl->n_light;
+    ctx->last.variant = pl->variant;
+    return NF_OK;
+}
+
+extern "C" nf_status nf_box_kick(nf_ctx *ctx, nf_box *box, int lo, int hi,
+                                 const nf_kick_params *kick, const float *far_acc, float *vel,
+                                 void *acc_out, float *cell_stats) {
+    if (!ctx || !box || !kick || !vel || lo < 0 || hi > box->cpd || lo >= hi) {
+        set_error("nf_box_kick: bad argument");
+        return NF_EINVAL;
+    }
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    NF_CUDA(cudaSetDevice(ctx->device));
+    Plan *pl = nullptr;
+    nf_status st = get_plan(ctx, box, lo, hi, &pl);
+    if (st != NF_OK) return st;
+    cudaStream_t s = ctx->stream;
+    const nf_config &cfg = ctx->cfg;
+    cudaEventRecord(ctx->ev[3], s);
+    st = enqueue_pencil(ctx, box, *pl, s, cudaEventRecordDefault);
+    if (st != NF_OK) return st;
+    const int64_t c2 = (int64_t)box->cpd * box->cpd;
+    KickConst k{kick->near_scale, kick->rescale, kick->kick1, kick->kick2, kick->b2};
+    if (pl->n_range > 0 || cell_stats) {
+        kick_kernel<<<ctx->sms * 8, 256, 0, s>>>(
+            box->d_part, pl->n_range, 2 * cfg.near_field_radius + 1, cfg.b2 > 0.f ? 4 : 3,
+            output_scale(cfg, box->eps), box->d_cs, (int64_t)lo * c2, (int64_t)(hi - lo) * c2,
+            pl->p0, box->d_perm, k, far_acc, vel, acc_out, cfg.out_kind, cell_stats);
+        NF_CUDA(cudaGetLastError());
+    }
+    NF_CUDA(cudaEventRecord(ctx->ev[2], s));
+    NF_CUDA(cudaStreamSynchronize(s));
+    float k_ms = 0, c_ms = 0, t_ms = 0;
+    cudaEventElapsedTime(&k_ms, ctx->ev[0], ctx->ev[1]);
+    cudaEventElapsedTime(&c_ms, ctx->ev[1], ctx->ev[2]);
+    cudaEventElapsedTime(&t_ms, ctx->ev[3], ctx->ev[2]);
+    ctx->last.kernel_ms = k_ms;
+    ctx->last.coadd_ms = c_ms;
+    ctx->last.total_ms = t_ms;
+    ctx->last.pairs = pl->pairs;
+    ctx->last.padded_pairs = pl->padded_pairs;
+    ctx->last.launches = (pl->n_heavy_groups + pl->n_light > 0 ? 1 : 0) + 1;
     ctx->last.items = pl->n_heavy_groups * WARPS_PER_CTA + pl->n_light;
     ctx->last.variant = pl->variant;
     return NF_OK;

@@ -291,6 +291,13 @@ nf_status nf_box_create(nf_ctx *ctx, int cpd, int64_t np, const int64_t *cell_st
 nf_status nf_box_update(nf_ctx *ctx, nf_box *box, const float *x, const float *y,
                         const float *z);
 void nf_box_destroy(nf_ctx *ctx, nf_box *box);
+/* The same positions as records of three floats per particle (abacus'
+ * PosSlab / posstruct layout, cell order) instead of three arrays: the
+ * transpose to the device layout happens on the device (the reference
+ * transposes on the host into PosXYZ, singlestep/Timestep/pipeline.cpp:
+ * 84-124, singlestep/DataModel/cellparticles.cpp:214-226).  Host or device
+ * memory. */
+nf_status nf_box_update_aos(nf_ctx *ctx, nf_box *box, const float *xyz);
 /* Give the box its own softening parameter (same convention as
  * nf_config.eps for the context's softening; 0 = the context's), so that
  * boxes of different particle spacing share one context and one server.
@@ -396,6 +403,30 @@ nf_status nf_server_stats_get(nf_server *srv, nf_server_stats *stats);
 nf_status nf_server_stats_reset(nf_server *srv);
 /* Drain or cancel what is queued, wait for what runs (bounded), stop. */
 void nf_server_stop(nf_server *srv);
+
+/* Near field of slabs [lo, hi) fused with the step that follows it in
+ * abacus: RescaleAndCoAddAcceleration (singlestep/Timestep/kick.cpp:72-107)
+ * and KickCell (kick.cpp:30-56), per particle in float, unfused, in the
+ * reference's order:
+ *     a = (nacc * near_scale + far_acc) * rescale;   w = nacc.w - b2
+ *     v += a * kick1;  (cell stats);  v += a * kick2
+ * where nacc is the record nf_box_forces returns.  Device pointers, one
+ * record per particle of the slabs in particle order: far_acc float3 (NULL:
+ * no far field), vel float3 (updated in place), acc_out accstruct (out_kind;
+ * NULL: not stored), cell_stats 3 floats per cell of the slabs in cell
+ * order (NULL: not computed): mean square velocity after the first half
+ * kick, max |v| component, max |a| component (the cellinfo fields
+ * mean_square_velocity, max_component_velocity, max_component_acceleration;
+ * the mean is summed in a different order than the reference's loop). */
+typedef struct nf_kick_params {
+    float near_scale; /* single spline: 1/eps_int^3 (kick.cpp:86-96); otherwise 1 */
+    float rescale;    /* -3 (Omega_M - Omega_Smooth) / (8 pi N), negated for glass */
+    float kick1, kick2;
+    float b2;         /* WriteState.DensityKernelRad2, subtracted from w */
+} nf_kick_params;
+nf_status nf_box_kick(nf_ctx *ctx, nf_box *box, int slab_lo, int slab_hi,
+                      const nf_kick_params *kick, const float *far_acc, float *vel,
+                      void *acc_out, float *cell_stats);
 
 /* Allocation-free variant of the batched sweep (no counterpart in the
  * reference).  For callers that cannot call cudaMalloc -- code that runs

@@ -171,3 +171,33 @@ def host_threads() -> int:
         return len(os.sched_getaffinity(0))
     except AttributeError:  # pragma: no cover
         return os.cpu_count() or 1
+
+
+# ---------------------------------------------------------------------------
+# the step after the near field (test restatement of the reference's kick)
+# ---------------------------------------------------------------------------
+
+def rescale_and_kick(nacc, far, vel, counts, near_scale, rescale, kick1, kick2, b2=0.0):
+    """RescaleAndCoAddAcceleration (singlestep/Timestep/kick.cpp:72-107) then
+    KickCell (kick.cpp:30-56), in float32 and in the reference's operation
+    order, on particles in cell order (counts: particles per cell).
+
+    Returns (acc (N, 4): a and w = nacc.w - b2, the velocities after both half
+    kicks, per-cell stats (ncell, 3): mean square velocity after the first
+    half kick, max |v| component, max |a| component)."""
+    f = np.float32
+    nacc = np.asarray(nacc, np.float32)
+    a = (nacc[:, :3] * f(near_scale) + np.asarray(far, np.float32)) * f(rescale)
+    w = nacc[:, 3] - f(b2) if nacc.shape[1] == 4 else np.zeros(len(nacc), np.float32)
+    v1 = np.asarray(vel, np.float32) + a * f(kick1)
+    v2 = v1 + a * f(kick2)
+    counts = np.asarray(counts, np.int64)
+    ncell = counts.size
+    stats = np.zeros((ncell, 3), np.float32)
+    nz = counts > 0
+    starts = np.concatenate([[0], np.cumsum(counts)[:-1]])[nz]
+    n2 = (v1[:, 0] * v1[:, 0] + v1[:, 1] * v1[:, 1]) + v1[:, 2] * v1[:, 2]
+    stats[nz, 0] = np.add.reduceat(n2, starts) / counts[nz].astype(np.float32)
+    stats[nz, 1] = np.maximum.reduceat(np.abs(v1).max(axis=1), starts)
+    stats[nz, 2] = np.maximum.reduceat(np.abs(a).max(axis=1), starts)
+    return np.concatenate([a, w[:, None]], axis=1), v2, stats

@@ -1,0 +1,65 @@
+"""The steps either side of the near field, on the device: positions given
+as (x, y, z) records (nf_box_update_aos), and the near field fused with the
+rescale / co-add with the far field and the two half kicks (nf_box_kick),
+checked against the sweep plus the oracle's restatement of
+singlestep/Timestep/kick.cpp."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def kbox(synth):
+    return synth.clustered_box(70000, 15, seed=33, n_clumps=25)
+
+
+def test_aos_upload_equals_soa(capi, synth, kbox):
+    eps = synth.kernel_eps(1, synth.plummer_eps(41))
+    with capi.Context(softening=1, eps=eps, kernel_variant=0) as ctx:
+        a = ctx.box(kbox)
+        want = a.forces()
+        b = ctx.box(kbox)
+        b.update_aos(np.stack([kbox.x, kbox.y, kbox.z], axis=1))
+        got = b.forces()
+        a.close()
+        b.close()
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+
+
+@pytest.mark.parametrize("softening", [0, 1])
+def test_kick_matches_sweep_plus_reference_kick(capi, synth, oracle, kbox, softening):
+    import torch
+    lo, hi = 3, 11
+    eps = synth.kernel_eps(softening, synth.plummer_eps(41))
+    L_int = synth.plummer_eps(41) * (synth.SINGLE_SPLINE_FACTOR if softening == 1 else 1.0)
+    near_scale = np.float32(1.0 / L_int ** 3) if softening == 1 else np.float32(1.0)
+    rescale = np.float32(-3.0 * (0.31 - 0.0) / (8.0 * np.pi * kbox.n))
+    k1, k2 = np.float32(0.013), np.float32(0.011)
+    p0, p1 = kbox.slab_range(lo)[0], kbox.slab_range(hi - 1)[1]
+    n = p1 - p0
+    rng = np.random.default_rng(4)
+    far = (rng.standard_normal((n, 3)) * 1e3).astype(np.float32)
+    vel = (rng.standard_normal((n, 3)) * 1e-2).astype(np.float32)
+    c2 = kbox.cpd ** 2
+    counts = kbox.counts[lo * c2:hi * c2]
+    with capi.Context(softening=softening, eps=eps) as ctx:
+        db = ctx.box(kbox)
+        nacc = db.forces(lo, hi)
+        d_far = torch.from_numpy(far).cuda()
+        d_vel = torch.from_numpy(vel).cuda()
+        d_acc = torch.empty((n, 4), dtype=torch.float32, device="cuda")
+        d_st = torch.empty(((hi - lo) * c2, 3), dtype=torch.float32, device="cuda")
+        for rep in range(2):  # twice: the second call starts from the kicked velocities
+            v_in = d_vel.cpu().numpy()
+            db.kick(lo, hi, d_vel.data_ptr(), d_far.data_ptr(), d_acc.data_ptr(), d_st.data_ptr(),
+                    near_scale=float(near_scale), rescale=float(rescale), kick1=float(k1),
+                    kick2=float(k2))
+            acc_w, v_w, st_w = oracle.rescale_and_kick(nacc, far, v_in, counts, near_scale,
+                                                       rescale, k1, k2)
+            assert np.array_equal(d_acc.cpu().numpy().view(np.uint32), acc_w.view(np.uint32))
+            assert np.array_equal(d_vel.cpu().numpy().view(np.uint32), v_w.view(np.uint32))
+            st = d_st.cpu().numpy()
+            assert np.array_equal(st[:, 1:], st_w[:, 1:])  # maxima: exact
+            np.testing.assert_allclose(st[:, 0], st_w[:, 0], rtol=1e-5, atol=0)
+        db.close()
