@@ -149,6 +149,8 @@ class KickParams(ctypes.Structure):
 # Every symbol the header declares; the loader checks each one is exported.
 EXPORTS = {
     "nf_box_update_aos": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "nf_box_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                   ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]),
     "nf_box_kick": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
                                    ctypes.POINTER(KickParams), ctypes.c_void_p, ctypes.c_void_p,
                                    ctypes.c_void_p, ctypes.c_void_p]),
@@ -333,6 +335,12 @@ class DeviceBox:
 
     def update(self, x, y, z):
         check(lib().nf_box_update(self.ctx.h, self.h, _ptr(x), _ptr(y), _ptr(z)), "nf_box_update")
+
+    def step(self, x, y, z, out: np.ndarray, n_chunks: int = 0):
+        """Upload + full sweep + download, pipelined over slab chunks (host arrays)."""
+        check(lib().nf_box_step(self.ctx.h, self.h, _ptr(x), _ptr(y), _ptr(z), _ptr(out), n_chunks),
+              "nf_box_step")
+        return out
 
     def update_aos(self, xyz):
         """New positions as (N, 3) float32 records (host array or device pointer)."""

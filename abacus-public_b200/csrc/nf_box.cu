@@ -549,10 +549,11 @@ __device__ __forceinline__ uint32_t cell_coord10(float u, int cpd) {
 // arrays; 3: one array of (x, y, z) records).
 __global__ void order_keys(const float *__restrict__ x, const float *__restrict__ y,
                            const float *__restrict__ z, int comp_stride,
-                           const int64_t *__restrict__ cs, int64_t ncell, int cpd, int64_t n,
-                           uint64_t *key, uint32_t *val) {
+                           const int64_t *__restrict__ cs, int64_t ncell, int cpd, int64_t p_begin,
+                           int64_t p_end, uint64_t *key, uint32_t *val) {
     int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride) {
+    for (int64_t p = p_begin + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < p_end;
+         p += stride) {
         // cell of particle p: the last c with cs[c] <= p
         int64_t lo = 0, hi = ncell;  // cs[lo] <= p < cs[hi]
         while (hi - lo > 1) {
@@ -571,9 +572,11 @@ __global__ void order_keys(const float *__restrict__ x, const float *__restrict_
 
 __global__ void pack_ordered(const float *__restrict__ x, const float *__restrict__ y,
                              const float *__restrict__ z, int comp_stride,
-                             const uint32_t *__restrict__ perm, int64_t n, float4 *out) {
+                             const uint32_t *__restrict__ perm, int64_t p_begin, int64_t p_end,
+                             float4 *out) {
     int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride) {
+    for (int64_t p = p_begin + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < p_end;
+         p += stride) {
         int64_t q = (int64_t)perm[p] * comp_stride;
         out[p] = make_float4(x[q], y[q], z[q], 0.f);
     }
@@ -1037,6 +1040,28 @@ static nf_status enqueue_forces(nf_ctx *ctx, nf_box *box, Plan &pl, cudaStream_t
     return NF_OK;
 }
 
+// The plan's CUDA graph (pencil kernel + co-add), captured on first use.
+static nf_status ensure_graph(nf_ctx *ctx, nf_box *box, Plan &pl) {
+    if (pl.graph) return NF_OK;
+    cudaStream_t s = ctx->stream;
+    cudaGraph_t g = nullptr;
+    NF_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    nf_status est = enqueue_forces(ctx, box, pl, s);
+    cudaError_t ce = cudaStreamEndCapture(s, &g);
+    if (est != NF_OK) {
+        if (g) cudaGraphDestroy(g);
+        return est;
+    }
+    if (ce != cudaSuccess) return cuda_fail(ce, "cudaStreamEndCapture");
+    ce = cudaGraphInstantiate(&pl.graph, g, 0);
+    cudaGraphDestroy(g);
+    if (ce != cudaSuccess) {
+        pl.graph = nullptr;
+        return cuda_fail(ce, "cudaGraphInstantiate");
+    }
+    return NF_OK;
+}
+
 }  // namespace nf
 
 using namespace nf;
@@ -1128,12 +1153,20 @@ extern "C" nf_status nf_box_update_aos(nf_ctx *ctx, nf_box *box, const float *xy
     return box_upload(ctx, box, nullptr, nullptr, nullptr, xyz);
 }
 
-static nf_status nf::box_upload(nf_ctx *ctx, nf_box *box, const float *x, const float *y,
-                                const float *z, const float *aos) {
-    NF_CUDA(cudaSetDevice(ctx->device));
-    // stage the three components through the box's device staging buffer
-    size_t bytes = (size_t)box->np * sizeof(float);
-    if (!box->d_stage && box->np > 0) {
+namespace nf {
+// Staging buffer, ordering scratch and permutation of a box (allocated once).
+struct OrderScratch {
+    uint64_t *k_in, *k_out;
+    uint32_t *v_in;
+    void *temp;
+    size_t temp_bytes;
+    int key_bits;
+};
+
+static nf_status upload_scratch(nf_ctx *ctx, nf_box *box, OrderScratch &o) {
+    const int64_t n = box->np;
+    const size_t bytes = (size_t)n * sizeof(float);
+    if (!box->d_stage && n > 0) {
         if (cudaMalloc(&box->d_stage, 3 * bytes) != cudaSuccess) {
             cudaGetLastError();
             box->d_stage = nullptr;
@@ -1141,19 +1174,16 @@ static nf_status nf::box_upload(nf_ctx *ctx, nf_box *box, const float *x, const 
             return NF_ENOMEM;
         }
     }
-    const int64_t n = box->np;
     const int64_t ncell = (int64_t)box->cpd * box->cpd * box->cpd;
-    // in-cell ordering scratch: keys in/out, values in, radix-sort temp; the
-    // sorted values are the box's permutation
-    int key_bits = 30;
-    while (key_bits < 64 && ((uint64_t)1 << (key_bits - 30)) < (uint64_t)ncell) key_bits++;
-    size_t temp = 0;
+    o.key_bits = 30;
+    while (o.key_bits < 64 && ((uint64_t)1 << (o.key_bits - 30)) < (uint64_t)ncell) o.key_bits++;
+    o.temp_bytes = 0;
     cudaError_t e = cub::DeviceRadixSort::SortPairs(
-        nullptr, temp, (const uint64_t *)nullptr, (uint64_t *)nullptr, (const uint32_t *)nullptr,
-        (uint32_t *)nullptr, (int)n, 0, key_bits, ctx->stream);
+        nullptr, o.temp_bytes, (const uint64_t *)nullptr, (uint64_t *)nullptr,
+        (const uint32_t *)nullptr, (uint32_t *)nullptr, (int)n, 0, o.key_bits, ctx->stream);
     if (e != cudaSuccess) return cuda_fail(e, "box upload (ordering size query)");
     const size_t kb = ((size_t)n * 8 + 255) & ~(size_t)255, vb = ((size_t)n * 4 + 255) & ~(size_t)255;
-    const size_t need = 2 * kb + vb + temp;
+    const size_t need = 2 * kb + vb + o.temp_bytes;
     if (box->sort_bytes < need) {
         cudaFree(box->d_sort);
         box->d_sort = nullptr;
@@ -1173,15 +1203,48 @@ static nf_status nf::box_upload(nf_ctx *ctx, nf_box *box, const float *x, const 
         return NF_ENOMEM;
     }
     unsigned char *sb = (unsigned char *)box->d_sort;
-    uint64_t *k_in = (uint64_t *)sb, *k_out = (uint64_t *)(sb + kb);
-    uint32_t *v_in = (uint32_t *)(sb + 2 * kb);
-    void *d_temp = sb + 2 * kb + vb;
+    o.k_in = (uint64_t *)sb;
+    o.k_out = (uint64_t *)(sb + kb);
+    o.v_in = (uint32_t *)(sb + 2 * kb);
+    o.temp = sb + 2 * kb + vb;
+    return NF_OK;
+}
+
+// Order the staged particles [p0, p1) inside their cells and pack them into
+// the box (the range must hold whole cells).  Components at x/y/z with
+// stride cstride.
+static cudaError_t order_range(nf_ctx *ctx, nf_box *box, const OrderScratch &o, const float *x,
+                               const float *y, const float *z, int cstride, int64_t p0,
+                               int64_t p1, cudaStream_t st) {
+    if (p1 <= p0) return cudaSuccess;
+    const int64_t ncell = (int64_t)box->cpd * box->cpd * box->cpd;
+    order_keys<<<ctx->sms * 8, 256, 0, st>>>(x, y, z, cstride, box->d_cs, ncell, box->cpd, p0, p1,
+                                             o.k_in, o.v_in);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    size_t tb = o.temp_bytes;
+    e = cub::DeviceRadixSort::SortPairs(o.temp, tb, o.k_in + p0, o.k_out + p0, o.v_in + p0,
+                                        box->d_perm + p0, (int)(p1 - p0), 0, o.key_bits, st);
+    if (e != cudaSuccess) return e;
+    pack_ordered<<<ctx->sms * 8, 256, 0, st>>>(x, y, z, cstride, box->d_perm, p0, p1, box->d_pos);
+    return cudaGetLastError();
+}
+}  // namespace nf
+
+static nf_status nf::box_upload(nf_ctx *ctx, nf_box *box, const float *x, const float *y,
+                                const float *z, const float *aos) {
+    NF_CUDA(cudaSetDevice(ctx->device));
+    OrderScratch o;
+    nf_status ost = upload_scratch(ctx, box, o);
+    if (ost != NF_OK) return ost;
+    const int64_t n = box->np;
+    const size_t bytes = (size_t)n * sizeof(float);
     float *tmp = box->d_stage;
     cudaStream_t st = ctx->stream;
     // staged components: SoA at tmp, tmp + n, tmp + 2n (stride 1) or the
     // AoS records as given at tmp, tmp + 1, tmp + 2 (stride 3)
     const float *sx = tmp, *sy = aos ? tmp + 1 : tmp + n, *sz = aos ? tmp + 2 : tmp + 2 * n;
-    const int cstride = aos ? 3 : 1;
+    cudaError_t e;
     if (aos) {
         e = cudaMemcpyAsync(tmp, aos, 3 * bytes, cudaMemcpyDefault, st);
     } else {
@@ -1189,18 +1252,7 @@ static nf_status nf::box_upload(nf_ctx *ctx, nf_box *box, const float *x, const 
         if (e == cudaSuccess) e = cudaMemcpyAsync(tmp + n, y, bytes, cudaMemcpyDefault, st);
         if (e == cudaSuccess) e = cudaMemcpyAsync(tmp + 2 * n, z, bytes, cudaMemcpyDefault, st);
     }
-    if (e == cudaSuccess) {
-        order_keys<<<ctx->sms * 8, 256, 0, st>>>(sx, sy, sz, cstride, box->d_cs, ncell, box->cpd, n,
-                                                 k_in, v_in);
-        e = cudaGetLastError();
-    }
-    if (e == cudaSuccess)
-        e = cub::DeviceRadixSort::SortPairs(d_temp, temp, k_in, k_out, v_in, box->d_perm, (int)n, 0,
-                                            key_bits, st);
-    if (e == cudaSuccess) {
-        pack_ordered<<<ctx->sms * 8, 256, 0, st>>>(sx, sy, sz, cstride, box->d_perm, n, box->d_pos);
-        e = cudaGetLastError();
-    }
+    if (e == cudaSuccess) e = order_range(ctx, box, o, sx, sy, sz, aos ? 3 : 1, 0, n, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return cuda_fail(e, "nf_box_update");
     return NF_OK;
@@ -1216,6 +1268,9 @@ extern "C" void nf_box_destroy(nf_ctx *ctx, nf_box *box) {
     cudaFree(box->d_stage);
     cudaFree(box->d_perm);
     cudaFree(box->d_sort);
+    if (box->s_in) cudaStreamDestroy(box->s_in);
+    if (box->s_out) cudaStreamDestroy(box->s_out);
+    for (cudaEvent_t e : box->step_ev) cudaEventDestroy(e);
     delete box;
 }
 
@@ -1408,25 +1463,9 @@ extern "C" nf_status nf_box_forces(nf_ctx *ctx, nf_box *box, int lo, int hi, voi
     NF_CUDA(cudaSetDevice(ctx->device));
     Plan *pl = nullptr;
     nf_status st = get_plan(ctx, box, lo, hi, &pl);
+    if (st == NF_OK) st = ensure_graph(ctx, box, *pl);
     if (st != NF_OK) return st;
     cudaStream_t s = ctx->stream;
-    if (!pl->graph) {
-        cudaGraph_t g = nullptr;
-        NF_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-        nf_status est = enqueue_forces(ctx, box, *pl, s);
-        cudaError_t ce = cudaStreamEndCapture(s, &g);
-        if (est != NF_OK) {
-            if (g) cudaGraphDestroy(g);
-            return est;
-        }
-        if (ce != cudaSuccess) return cuda_fail(ce, "cudaStreamEndCapture");
-        ce = cudaGraphInstantiate(&pl->graph, g, 0);
-        cudaGraphDestroy(g);
-        if (ce != cudaSuccess) {
-            pl->graph = nullptr;
-            return cuda_fail(ce, "cudaGraphInstantiate");
-        }
-    }
     cudaEventRecord(ctx->ev[3], s);
     NF_CUDA(cudaGraphLaunch(pl->graph, s));
     NF_CUDA(cudaMemcpyAsync(out, pl->d_out, pl->out_bytes,
@@ -1487,6 +1526,106 @@ extern "C" nf_status nf_box_kick(nf_ctx *ctx, nf_box *box, int lo, int hi,
     ctx->last.launches = (pl->n_heavy_groups + pl->n_light > 0 ? 1 : 0) + 1;
     ctx->last.items = pl->n_heavy_groups * WARPS_PER_CTA + pl->n_light;
     ctx->last.variant = pl->variant;
+    return NF_OK;
+}
+
+extern "C" nf_status nf_box_step(nf_ctx *ctx, nf_box *box, const float *x, const float *y,
+                                 const float *z, void *out, int n_chunks) {
+    if (!ctx || !box || !out || (box->np > 0 && (!x || !y || !z))) {
+        set_error("nf_box_step: null argument");
+        return NF_EINVAL;
+    }
+    const int cpd = box->cpd, R = ctx->cfg.near_field_radius;
+    int K = n_chunks > 0 ? n_chunks : 8;
+    K = std::max(1, std::min(K, cpd / std::max(R, 1)));
+    if (n_chunks > 0 && K != n_chunks) {
+        set_error("nf_box_step: every chunk needs at least R slabs");
+        return NF_EINVAL;
+    }
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    NF_CUDA(cudaSetDevice(ctx->device));
+    // chunk bounds (slabs) and the plans of the chunk ranges
+    std::vector<int> b(K + 1);
+    for (int k = 0; k <= K; k++) b[k] = (int)((int64_t)cpd * k / K);
+    std::vector<Plan *> pls(K);
+    for (int k = 0; k < K; k++) {  // all plans first: a new plan may regrow the partials
+        nf_status st = get_plan(ctx, box, b[k], b[k + 1], &pls[k]);
+        if (st != NF_OK) return st;
+    }
+    for (int k = 0; k < K; k++) {
+        nf_status st = ensure_graph(ctx, box, *pls[k]);
+        if (st != NF_OK) return st;
+    }
+    OrderScratch o;
+    nf_status ost = upload_scratch(ctx, box, o);
+    if (ost != NF_OK) return ost;
+    if (!box->s_in) NF_CUDA(cudaStreamCreateWithFlags(&box->s_in, cudaStreamNonBlocking));
+    if (!box->s_out) NF_CUDA(cudaStreamCreateWithFlags(&box->s_out, cudaStreamNonBlocking));
+    while ((int)box->step_ev.size() < 2 * K + 2) {
+        cudaEvent_t e;
+        NF_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        box->step_ev.push_back(e);
+    }
+    cudaEvent_t *ev_in = box->step_ev.data(), *ev_out = ev_in + K, ev_go = ev_in[2 * K],
+                ev_done = ev_in[2 * K + 1];
+    cudaStream_t sc = ctx->stream, si = box->s_in, so = box->s_out;
+    const int64_t c2 = (int64_t)cpd * cpd, n = box->np;
+    auto P = [&](int slab) { return box->cell_start[(int64_t)slab * c2]; };
+    const size_t rec = ctx->cfg.out_kind == NF_OUT_FLOAT4 ? 16 : 12;
+    float *tmp = box->d_stage;
+    // copies in on s_in, ordering and sweeps on the context stream, copies
+    // out on s_out; the context stream waits for both at the end
+    NF_CUDA(cudaEventRecord(ev_go, sc));
+    NF_CUDA(cudaStreamWaitEvent(si, ev_go, 0));
+    NF_CUDA(cudaStreamWaitEvent(so, ev_go, 0));
+    for (int k = 0; k < K; k++) {
+        const int64_t p0 = P(b[k]), m = P(b[k + 1]) - p0;
+        if (m > 0) {
+            const size_t by = (size_t)m * sizeof(float);
+            NF_CUDA(cudaMemcpyAsync(tmp + p0, x + p0, by, cudaMemcpyDefault, si));
+            NF_CUDA(cudaMemcpyAsync(tmp + n + p0, y + p0, by, cudaMemcpyDefault, si));
+            NF_CUDA(cudaMemcpyAsync(tmp + 2 * n + p0, z + p0, by, cudaMemcpyDefault, si));
+        }
+        NF_CUDA(cudaEventRecord(ev_in[k], si));
+    }
+    auto sweep = [&](int k) -> nf_status {
+        // range k: its halo chunks are ordered already (stream order on sc)
+        NF_CUDA(cudaGraphLaunch(pls[k]->graph, sc));
+        NF_CUDA(cudaEventRecord(ev_out[k], sc));
+        NF_CUDA(cudaStreamWaitEvent(so, ev_out[k], 0));
+        if (pls[k]->out_bytes)
+            NF_CUDA(cudaMemcpyAsync((char *)out + (size_t)(P(b[k]) - P(0)) * rec, pls[k]->d_out,
+                                    pls[k]->out_bytes, cudaMemcpyDefault, so));
+        return NF_OK;
+    };
+    for (int k = 0; k < K; k++) {
+        NF_CUDA(cudaStreamWaitEvent(sc, ev_in[k], 0));
+        cudaError_t e = order_range(ctx, box, o, tmp, tmp + n, tmp + 2 * n, 1, P(b[k]),
+                                    P(b[k + 1]), sc);
+        if (e != cudaSuccess) return cuda_fail(e, "nf_box_step (ordering)");
+        if (k >= 2) {  // range k-1 has both halos: chunks k-2 and k
+            nf_status st = sweep(k - 1);
+            if (st != NF_OK) return st;
+        }
+    }
+    // the ranges next to the periodic wrap need the last chunk
+    if (K >= 2) {
+        nf_status st = sweep(K - 1);
+        if (st != NF_OK) return st;
+    }
+    nf_status st = sweep(0);
+    if (st != NF_OK) return st;
+    NF_CUDA(cudaEventRecord(ev_done, so));
+    NF_CUDA(cudaStreamWaitEvent(sc, ev_done, 0));
+    NF_CUDA(cudaStreamSynchronize(sc));
+    uint64_t pairs = 0, padded = 0;
+    for (Plan *pl : pls) {
+        pairs += pl->pairs;
+        padded += pl->padded_pairs;
+    }
+    ctx->last.pairs = pairs;
+    ctx->last.padded_pairs = padded;
+    ctx->last.launches = 2 * K;
     return NF_OK;
 }
 

@@ -106,6 +106,9 @@ struct nf_box {
     uint32_t *d_perm = nullptr;       // caller's index of the particle in each packed slot
     void *d_sort = nullptr;           // in-cell ordering scratch (keys, values, sort temp)
     size_t sort_bytes = 0;
+    // pipelined step (nf_box_step): copy-in and copy-out streams, per-chunk events
+    cudaStream_t s_in = nullptr, s_out = nullptr;
+    std::vector<cudaEvent_t> step_ev;
     size_t part_bytes = 0;
     std::map<std::pair<int, int>, std::unique_ptr<nf::Plan>> plans;
     int variant = -1;       // kernel shape chosen by the autotuner (-1: not tuned yet)

@@ -506,16 +506,16 @@ def our_arm(args, w):
     hz = torch.from_numpy(box.z).pin_memory()
     hout = torch.empty((n, 4), dtype=torch.float32).pin_memory()
     xa, ya, za, oa = hx.numpy(), hy.numpy(), hz.numpy(), hout.numpy()
-    db.update(xa, ya, za)
-    db.forces(0, box.cpd, out=oa)
+    # one call per step: copies in, sweeps and copies out overlap over 8 slab
+    # chunks (nf_box_step); the first call builds the chunk plans
+    db.step(xa, ya, za, oa)
     barrier(world)
     torch.cuda.synchronize()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(args.steps):
-        db.update(xa, ya, za)
-        db.forces(0, box.cpd, out=oa)
+        db.step(xa, ya, za, oa)
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = barrier_max(e0.elapsed_time(e1) / args.steps, world)

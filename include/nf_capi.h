@@ -291,6 +291,17 @@ nf_status nf_box_create(nf_ctx *ctx, int cpd, int64_t np, const int64_t *cell_st
 nf_status nf_box_update(nf_ctx *ctx, nf_box *box, const float *x, const float *y,
                         const float *z);
 void nf_box_destroy(nf_ctx *ctx, nf_box *box);
+/* One whole step end to end, pipelined: upload new positions (host or
+ * device x, y, z, same cell counts), sweep every slab, and copy the
+ * records of all particles to out (host or device), as nf_box_update +
+ * nf_box_forces(0, cpd) would, but in n_chunks slab chunks (0: 8) so that
+ * copies in and out overlap the sweeps of other chunks: chunk k is copied
+ * in and ordered, then the slab range whose halo it completes is swept and
+ * copied out while the next chunks arrive.  Each chunk needs at least R
+ * slabs.  Results equal nf_box_forces(lo, hi) over the same chunk ranges,
+ * bit for bit. */
+nf_status nf_box_step(nf_ctx *ctx, nf_box *box, const float *x, const float *y, const float *z,
+                      void *out, int n_chunks);
 /* The same positions as records of three floats per particle (abacus'
  * PosSlab / posstruct layout, cell order) instead of three arrays: the
  * transpose to the device layout happens on the device (the reference

@@ -63,3 +63,29 @@ def test_kick_matches_sweep_plus_reference_kick(capi, synth, oracle, kbox, softe
             assert np.array_equal(st[:, 1:], st_w[:, 1:])  # maxima: exact
             np.testing.assert_allclose(st[:, 0], st_w[:, 0], rtol=1e-5, atol=0)
         db.close()
+
+
+@pytest.mark.parametrize("chunks", [1, 2, 3, 5])
+def test_pipelined_step_equals_chunked_sweeps(capi, synth, kbox, chunks):
+    """nf_box_step (upload + sweep + download overlapped over slab chunks)
+    returns, bit for bit, what nf_box_update + nf_box_forces over the same
+    chunk ranges return, from fresh positions each call."""
+    eps = synth.kernel_eps(1, synth.plummer_eps(41))
+    rng = np.random.default_rng(chunks)
+    with capi.Context(softening=1, eps=eps, kernel_variant=0) as ctx:
+        db = ctx.box(kbox)
+        for rep in range(2):
+            # positions moved inside their cells (same cell counts)
+            h = np.float32(0.5 / kbox.cpd)
+            x = np.clip(kbox.x + rng.normal(0, 1e-3 * h, kbox.n).astype(np.float32), -h * 0.999, h * 0.999)
+            y, z = kbox.y.copy(), kbox.z.copy()
+            x = np.ascontiguousarray(x, dtype=np.float32)
+            out = np.full((kbox.n, 4), np.nan, np.float32)
+            db.step(x, y, z, out, chunks)
+            db.update(x, y, z)
+            bnd = [kbox.cpd * k // chunks for k in range(chunks + 1)]
+            want = np.concatenate([db.forces(bnd[k], bnd[k + 1]) for k in range(chunks)])
+            assert np.array_equal(out.view(np.uint32), want.view(np.uint32)), (chunks, rep)
+        with pytest.raises(capi.NfError):
+            db.step(x, y, z, out, kbox.cpd)  # chunks of fewer than R slabs
+        db.close()
