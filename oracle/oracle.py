@@ -201,3 +201,126 @@ def rescale_and_kick(nacc, far, vel, counts, near_scale, rescale, kick1, kick2, 
     stats[nz, 1] = np.maximum.reduceat(np.abs(v1).max(axis=1), starts)
     stats[nz, 2] = np.maximum.reduceat(np.abs(a).max(axis=1), starts)
     return np.concatenate([a, w[:, None]], axis=1), v2, stats
+
+
+# ---------------------------------------------------------------------------
+# the reference's own GPU pencil kernel (oracle/_ref/libnfref_gpu_*.so,
+# compiled from singlestep/Direct/PencilKernel.cu by the Makefile), driven on
+# the reference's SIC layout (PencilOnPencil.cc:254-416, PencilPlan.cc:22-90,
+# 214-255) for one whole x-slab; a checker for the GPU tests
+# ---------------------------------------------------------------------------
+
+_GPU_SOFT = {0: "plummer", 1: "single_spline"}
+
+
+def have_ref_gpu(softening: int) -> bool:
+    return softening in _GPU_SOFT and (REF_DIR / f"libnfref_gpu_{_GPU_SOFT[softening]}.so").exists()
+
+
+_ref_gpu_libs = {}
+
+
+def ref_gpu_lib(softening: int):
+    if softening not in _ref_gpu_libs:
+        L = ctypes.CDLL(str(REF_DIR / f"libnfref_gpu_{_GPU_SOFT[softening]}.so"))
+        p = ctypes.c_void_p
+        i = ctypes.c_int
+        f = ctypes.c_float
+        L.nfrefgpu_run.argtypes = [i, i, p, p, p, i, p, i, p, p, i, p, p, f, f, i, p, p]
+        L.nfrefgpu_run.restype = i
+        L.nfrefgpu_accstruct_floats.restype = i
+        _ref_gpu_libs[softening] = L
+    return _ref_gpu_libs[softening]
+
+
+def _fill(box, cid, shift_col, sx, sy, sz, starts, shift):
+    """Copy the particles of cells cid[p, c] into slots starts[p] + running
+    offset, adding shift[c] to the coordinate shift_col (0: x, 2: z)."""
+    cs = box.cell_start
+    n = (cs[cid + 1] - cs[cid]).astype(np.int64)
+    P, W = cid.shape
+    off = np.zeros_like(n)
+    off[:, 1:] = np.cumsum(n, axis=1)[:, :-1]
+    dst0 = (starts[:, None] + off).ravel()
+    src0 = cs[cid].ravel()
+    nf = n.ravel()
+    tot = int(nf.sum())
+    pair = np.repeat(np.arange(nf.size), nf)
+    within = np.arange(tot) - np.repeat(np.cumsum(nf) - nf, nf)
+    src = src0[pair] + within
+    dst = dst0[pair] + within
+    sh = np.repeat(np.tile(shift, P), nf)
+    comp = [box.x, box.y, box.z]
+    for k, out in enumerate((sx, sy, sz)):
+        v = comp[k][src]
+        out[dst] = v + sh if k == shift_col else v
+    return src, dst
+
+
+def ref_gpu_slab(box, softening, eps, slab, repeats=1, b2=0.0, R=2):
+    """The reference GPU kernel on one whole x-slab as one SIC: returns
+    (acc float32[n_slab, 3] in particle order, mean launch ms, DirectTotal
+    pairs).  Sink pencil (y=j, z centre k): cells (slab, j, k-R..k+R) with z
+    shifted by (c-R) h; source pencil (j', k): cells (slab-R..slab+R, j', k)
+    with x shifted by (c-R) h; the y shift (y-R) h is applied on the device.
+    The five pencil partials of each sink are co-added in float32."""
+    f32 = np.float32
+    cpd, W = box.cpd, 2 * R + 1
+    h = f32(1.0 / cpd)
+    shift = np.array([f32(c - R) * h for c in range(W)], dtype=np.float32)
+    cs = box.cell_start
+    counts = np.diff(cs)
+    j = np.repeat(np.arange(cpd), cpd)
+    k = np.tile(np.arange(cpd), cpd)
+    P = cpd * cpd
+    cells = np.arange(W)
+    sink_cid = (slab * cpd + j[:, None]) * cpd + (k[:, None] + cells[None, :] - R) % cpd
+    n_p = counts[sink_cid].sum(axis=1)
+    padded = (n_p + 63) // 64 * 64
+    s_start = np.concatenate([[0], np.cumsum(padded)[:-1]]).astype(np.int64)
+    nslots = int(padded.sum())
+    sx = np.zeros(nslots, f32)
+    sy = np.zeros(nslots, f32)
+    sz = np.zeros(nslots, f32)
+    s_src, s_dst = _fill(box, sink_cid, 2, sx, sy, sz, s_start, shift)
+    id_max = (s_start + n_p).astype(np.uint32)
+    nblk = padded // 64
+    parent = np.repeat(np.arange(P), nblk).astype(np.int32)
+    src_cid = (((slab + cells[None, :] - R) % cpd) * cpd + j[:, None]) * cpd + k[:, None]
+    n_q = counts[src_cid].sum(axis=1)
+    q_start = np.concatenate([[0], np.cumsum(n_q)[:-1]]).astype(np.int64)
+    nsrc = int(n_q.sum())
+    tx = np.zeros(nsrc, f32)
+    ty = np.zeros(nsrc, f32)
+    tz = np.zeros(nsrc, f32)
+    _fill(box, src_cid, 0, tx, ty, tz, q_start, shift)
+    ys = np.arange(W)
+    ilist = (((j[:, None] + ys[None, :] - R) % cpd) * cpd + k[:, None]).astype(np.int32)
+    yoff = np.tile(shift, (P, 1)).astype(np.float32)
+    # every index the kernel will use, checked on the host before the launch
+    assert parent.size == nslots // 64
+    assert np.all(id_max <= nslots) and np.all(s_start % 64 == 0)
+    assert np.all((ilist >= 0) & (ilist < P))
+    assert np.all(q_start + n_q <= nsrc)
+    assert nslots < 2 ** 31 and nsrc < 2 ** 31
+    L = ref_gpu_lib(softening)
+    nf4 = L.nfrefgpu_accstruct_floats()
+    acc = np.zeros((max(nslots, 1), nf4), f32)
+    sink_xyz = np.ascontiguousarray(np.concatenate([sx, sy, sz]))
+    src_xyz = np.ascontiguousarray(np.concatenate([tx, ty, tz]))
+    q_start32 = q_start.astype(np.int32)
+    n_q32 = n_q.astype(np.int32)
+    ms = ctypes.c_float(0)
+    ptr = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+    rc = L.nfrefgpu_run(int(nblk.sum()), nslots, ptr(sink_xyz), ptr(id_max), ptr(parent), nsrc,
+                        ptr(src_xyz), P, ptr(q_start32), ptr(n_q32), int(ilist.size),
+                        ptr(np.ascontiguousarray(ilist.ravel())),
+                        ptr(np.ascontiguousarray(yoff.ravel())), float(np.float32(eps)),
+                        float(np.float32(b2)), int(repeats), ptr(acc), ctypes.byref(ms))
+    if rc != 0:
+        raise RuntimeError(f"reference GPU kernel failed: cudaError {rc}")
+    p0, p1 = box.slab_range(slab)
+    out = np.zeros((p1 - p0, 3), f32)
+    np.add.at(out, s_src - p0, acc[s_dst, :3])
+    pairs = int((n_p[:, None] * n_q[ilist]).sum())
+    return out, ms.value, pairs

@@ -1,0 +1,69 @@
+"""Against the reference's own GPU kernel: ComputeDirects
+(singlestep/Direct/PencilKernel.cu) compiled from the reference sources for
+sm_100a with its default GPU configuration (fast-math rsqrt without a
+Newton step, BLOCK_ACCUM, float accumulation; oracle/_ref, built by
+oracle/Makefile), driven on the reference's SIC layout for whole x-slabs.
+
+* parity: this library's slab forces agree with the reference kernel's
+  within the tolerance of the other tests (the reference kernel's own error
+  is ~1e-6);
+* the reference-kernel bar: pair interactions/s of the reference kernel on
+  the same GPU next to this library's batched sweep (printed; run with -s).
+  NF_REFKERNEL_WORKLOAD=clustered256 measures the default bench box.
+"""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("softening", [0, 1])
+def test_slabs_match_reference_gpu_kernel(capi, synth, oracle, softening):
+    if not oracle.have_ref_gpu(softening):
+        pytest.skip("reference GPU kernel not built (needs the reference sources)")
+    box = synth.clustered_box(60000, 13, seed=71, n_clumps=20)
+    eps = synth.kernel_eps(softening, synth.plummer_eps(39))
+    with capi.Context(softening=softening, eps=eps) as ctx:
+        db = ctx.box(box)
+        for slab in (0, 6, 12):
+            ref, _, pairs = oracle.ref_gpu_slab(box, softening, eps, slab)
+            got = db.forces(slab, slab + 1)[:, :3]
+            assert db.pair_count(slab, slab + 1) == pairs
+            norm = np.linalg.norm(ref.astype(np.float64), axis=1)
+            diff = np.abs(got.astype(np.float64) - ref)
+            ok = norm > 0
+            assert np.all(diff[ok] <= 1e-4 * norm[ok, None]), float((diff[ok] / norm[ok, None]).max())
+        db.close()
+
+
+def test_reference_kernel_bar(capi, synth, oracle):
+    if not oracle.have_ref_gpu(1):
+        pytest.skip("reference GPU kernel not built (needs the reference sources)")
+    sys.path.insert(0, str(os.path.dirname(os.path.dirname(os.path.abspath(__file__)))))
+    import bench
+    wl = os.environ.get("NF_REFKERNEL_WORKLOAD", "clustered128")
+    w = bench.WORKLOADS[wl]
+    box = bench.make_box(w)
+    eps = bench.kernel_eps(w)
+    soft = w["softening"]
+    ref_ms, ref_pairs = 0.0, 0
+    for slab in range(box.cpd):
+        _, ms, pairs = oracle.ref_gpu_slab(box, soft, eps, slab, repeats=2)
+        ref_ms += ms
+        ref_pairs += pairs
+    with capi.Context(softening=soft, eps=eps) as ctx:
+        db = ctx.box(box)
+        for _ in range(3):
+            db.forces()
+        ours_ms = min((db.forces(), ctx.last_timing().kernel_ms)[1] for _ in range(3))
+        pairs = db.pair_count()
+        db.close()
+    assert pairs == ref_pairs
+    ref_rate, ours_rate = ref_pairs / (ref_ms / 1e3), pairs / (ours_ms / 1e3)
+    print(f"\n[reference-kernel bar] {wl}: reference ComputeDirects (sm_100a, one SIC per slab) "
+          f"{ref_ms:.1f} ms = {ref_rate:.3e} pairs/s; this library's batched sweep "
+          f"{ours_ms:.1f} ms = {ours_rate:.3e} pairs/s; ratio {ours_rate / ref_rate:.2f}")
+    assert ours_rate > ref_rate
