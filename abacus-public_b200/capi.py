@@ -324,8 +324,10 @@ class DeviceBox:
         self.np = box.n
         self._cs = np.ascontiguousarray(box.cell_start, dtype=np.int64)
         h = ctypes.c_void_p()
-        check(lib().nf_box_create(ctx.h, box.cpd, box.n, _ptr(self._cs), _ptr(box.x), _ptr(box.y),
-                                  _ptr(box.z), ctypes.byref(h)), "nf_box_create")
+        # positions: numpy arrays (host) or torch tensors (host or device)
+        p = (lambda a: ctypes.c_void_p(a.data_ptr()) if hasattr(a, "data_ptr") else _ptr(a))
+        check(lib().nf_box_create(ctx.h, box.cpd, box.n, _ptr(self._cs), p(box.x), p(box.y),
+                                  p(box.z), ctypes.byref(h)), "nf_box_create")
         self.h = h
 
     def close(self):

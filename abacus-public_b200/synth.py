@@ -163,3 +163,70 @@ def kernel_eps(softening: int, length_plummer: float) -> float:
         return float(np.float32(1.0 / e))
     e = length_plummer
     return float(np.float32(e * e * e))
+
+
+def clustered_box_device(n: int, cpd: int, seed: int = 0, device="cuda", n_clumps: int = 2000,
+                         clump_fraction: float = 0.6, m_lo: float = 1e-5, m_hi: float = 1e-3,
+                         conc: float = 10.0, r_trunc_cells: float = 0.6, chunk: int = 1 << 26):
+    """The clustered mixture of clustered_box, generated on a GPU with torch
+    for boxes too large for host memory (10^9 particles): the same recipe
+    (clump masses, NFW radii, uniform background, binning in double, float32
+    cell-relative positions sorted by cell), a different random stream.
+    Returns (x, y, z) float32 device tensors in cell order and the host
+    cell_start (int64[cpd^3 + 1])."""
+    import torch
+    dev = torch.device(device)
+    rng = np.random.default_rng(seed)
+    n_clumped = int(round(clump_fraction * n))
+    raw = np.exp(rng.uniform(np.log(m_lo), np.log(m_hi), n_clumps)) * n
+    m = raw * (n_clumped / raw.sum())
+    mi = np.floor(m).astype(np.int64)
+    short = n_clumped - int(mi.sum())
+    if short > 0:
+        mi[np.argsort(m - mi)[::-1][:short]] += 1
+    centres = torch.from_numpy(rng.random((n_clumps, 3)) - 0.5).to(dev)
+    ends = torch.from_numpy(np.cumsum(mi)).to(dev)
+    xs = np.concatenate([[0.0], np.geomspace(1e-6, conc, 4096)])
+    mtab = np.log1p(xs) - xs / (1.0 + xs)
+    xs_t, m_t = torch.from_numpy(xs).to(dev), torch.from_numpy(mtab).to(dev)
+    r_s = (r_trunc_cells / cpd) / conc
+    g = torch.Generator(device=dev)
+    g.manual_seed(int(seed) * 7919 + 17)
+    half = (cpd - 1) // 2
+    h = 1.0 / cpd
+    hh = np.float32(0.5 * h)
+    hi_f = float(np.nextafter(hh, np.float32(0.0)))
+    cid = torch.empty(n, dtype=torch.int64, device=dev)
+    lf = torch.empty((3, n), dtype=torch.float32, device=dev)
+    for p0 in range(0, n, chunk):
+        p1 = min(n, p0 + chunk)
+        idx = torch.arange(p0, p1, device=dev)
+        gpos = torch.rand((p1 - p0, 3), generator=g, device=dev, dtype=torch.float64) - 0.5
+        cl = idx < n_clumped
+        if bool(cl.any()):
+            ic = idx[cl]
+            which = torch.searchsorted(ends, ic, right=True)
+            u = torch.rand(ic.numel(), generator=g, device=dev, dtype=torch.float64) * m_t[-1]
+            k = torch.clamp(torch.searchsorted(m_t, u), 1, m_t.numel() - 1)
+            t = (u - m_t[k - 1]) / (m_t[k] - m_t[k - 1])
+            r = (xs_t[k - 1] + t * (xs_t[k] - xs_t[k - 1])) * r_s
+            v = torch.randn((ic.numel(), 3), generator=g, device=dev, dtype=torch.float64)
+            v /= torch.linalg.norm(v, dim=1, keepdim=True)
+            gpos[cl] = centres[which] + v * r[:, None]
+        gpos -= torch.floor(gpos + 0.5)
+        c = torch.clamp(torch.floor((gpos + 0.5) * cpd).to(torch.int64), 0, cpd - 1)
+        local = (gpos - (c - half).to(torch.float64) * h).to(torch.float32)
+        local.clamp_(-float(hh), hi_f)
+        cid[p0:p1] = (c[:, 0] * cpd + c[:, 1]) * cpd + c[:, 2]
+        lf[:, p0:p1] = local.T
+        del gpos, c, local
+    counts = torch.bincount(cid, minlength=cpd ** 3).cpu().numpy()
+    _, order = torch.sort(cid, stable=True)
+    del cid
+    out = []
+    for k in range(3):
+        out.append(lf[k][order].contiguous())
+    del lf, order
+    cell_start = np.zeros(cpd ** 3 + 1, dtype=np.int64)
+    np.cumsum(counts, out=cell_start[1:])
+    return out[0], out[1], out[2], cell_start

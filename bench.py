@@ -61,6 +61,9 @@ WORKLOADS = {
                               "(the profiling case)"),
     "uniform256": dict(n_side=256, cpd=65, softening=0, kind="uniform", seed=5,
                        desc="256^3 uniform particles, cpd 65, Plummer eps=spacing/40"),
+    "clustered1024": dict(n_side=1024, cpd=255, softening=1, kind="clustered_device", seed=6,
+                          desc="1024^3 particles, cpd 255, clustered mixture as clustered256, "
+                               "generated on the GPU; a step sweeps a bounded range of slabs"),
 }
 
 
@@ -600,6 +603,82 @@ def our_arm(args, w):
     return 0
 
 
+def big_arm(args, w):
+    """The largest box (1024^3, generated on the GPU: it does not fit the
+    host-side generator).  A full sweep is ~5e14 pairs (minutes), so a step
+    sweeps the slab range [0, --slabs) as one persistent launch; value =
+    that range's pairs / device time.  The kernel shape is fixed (shape 0,
+    the one the autotuner picks on the 256^3 and 512^3 boxes): tuning would
+    cost five launches of the range.  Accuracy: the FP64 oracle on 2000
+    seeded sinks of the range; no CPU baseline (its sample would take
+    hours)."""
+    import torch
+    _pkg()
+    from abacus_public_b200 import capi, synth
+    torch.cuda.set_device(0)
+    n = w["n_side"] ** 3
+    x, y, z, cs = synth.clustered_box_device(n, w["cpd"], w["seed"], device="cuda")
+    hbox = synth.Box(w["cpd"], x.cpu().numpy(), y.cpu().numpy(), z.cpu().numpy(), cs, "clustered1024")
+    dbox = synth.Box(w["cpd"], x, y, z, cs, "clustered1024")
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    eps = kernel_eps(w)
+    ctx = capi.Context(softening=w["softening"], eps=eps, kernel_variant=0)
+    ctx.set_stream(stream.cuda_stream)
+    peak_b, peak_s = ctx.fp32_peak(1.0)
+    db = ctx.box(dbox)
+    del x, y, z, dbox
+    torch.cuda.empty_cache()
+    lo, hi = 0, min(args.slabs, w["cpd"])
+    p0, p1 = db.slab_particles(lo, hi)
+    out = torch.empty((p1 - p0, 4), dtype=torch.float32, device="cuda")
+    pairs = db.pair_count(lo, hi)
+    for _ in range(args.warmup):
+        db.forces_device(lo, hi, out.data_ptr())
+    torch.cuda.synchronize()
+    kms = []
+    with ClockSampler(0) as clk:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            db.forces_device(lo, hi, out.data_ptr())
+            kms.append(ctx.last_timing().kernel_ms)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    t = ctx.last_timing()
+    k_ms = float(np.mean(kms))
+    flops = FLOPS_PER_PAIR[w["softening"]]
+    achieved = pairs * flops / (k_ms / 1e3) / 1e12
+    res = out.cpu().numpy()
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+    sinks = np.sort(np.random.default_rng(5).choice(np.arange(p0, p1), 2000, replace=False))
+    rms, mx, _ = oracle.frac_errors(res[sinks - p0, :3], oracle.fp64_sinks(hbox, w["softening"], eps, sinks))
+    counts = np.diff(cs)
+    result = {
+        "metric": "pair_interactions_per_s", "value": pairs / (ms / 1e3), "unit": "pairs/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (generated on the GPU)",
+        "config": {"workload": args.workload, "desc": w["desc"], "particles": n, "cpd": w["cpd"],
+                   "slabs": [lo, hi], "particles_in_slabs": p1 - p0, "pairs_per_step": pairs,
+                   "padded_pairs_per_step": int(t.padded_pairs),
+                   "max_particles_per_cell": int(counts.max()), "kernel_shape": 0},
+        "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak_s, "unit": "TFLOP/s",
+                     "frac": achieved / peak_s, "traffic": None, "kernel": "pencil_kernel",
+                     "kernel_ms": k_ms, "flops_per_pair": flops},
+        "accuracy_vs_fp64": {"rms_frac": rms, "max_frac": mx, "sinks": 2000},
+        "gpu_launches": int(args.steps * t.launches),
+        "clocks": clk.summary(),
+        "device_bytes": db.device_bytes() if hasattr(db, "device_bytes") else None,
+    }
+    db.close()
+    ctx.close()
+    print(json.dumps(result), flush=True)
+    return 0
+
+
 def shard_arm(args, w):
     """One box split over the ranks (strong scaling): contiguous x-slab
     ranges balanced by pair count, a 2-slab position halo exchanged per step
@@ -723,6 +802,8 @@ def main():
     ap.add_argument("--precision-study", action="store_true",
                     help="also sweep with plain FP32 accumulation and compare both with the "
                          "FP64 oracle on 0.1%% of the sinks")
+    ap.add_argument("--slabs", type=int, default=32,
+                    help="clustered1024: the slab range [0, SLABS) a step sweeps")
     ap.add_argument("--shard", action="store_true",
                     help="split one box over the ranks (strong scaling, 2-slab halo exchange) "
                          "instead of one independent box per rank")
@@ -737,6 +818,8 @@ def main():
         return reference_arm(args, w)
     if args.shard:
         return shard_arm(args, w)
+    if w["kind"] == "clustered_device":
+        return big_arm(args, w)
     return our_arm(args, w)
 
 
