@@ -28,3 +28,20 @@ def test_kernel_eps(synth):
     assert abs(e - 1 / 64 / 40) < 1e-15
     assert synth.kernel_eps(0, e) == np.float32(e * e)
     assert synth.kernel_eps(1, e) == np.float32(1 / (e * 2.15517) ** 2)
+
+
+def test_device_generator_layout(synth):
+    """The GPU generator (run here on CPU tensors) keeps the box layout:
+    cell order, counts summing to n, positions inside their cells, the
+    clumped fraction visible as crowded cells, and a fixed seed."""
+    x, y, z, cs = synth.clustered_box_device(60000, 13, seed=4, device="cpu", chunk=1 << 14)
+    assert x.shape[0] == 60000 and cs[-1] == 60000 and cs[0] == 0
+    assert np.all(np.diff(cs) >= 0)
+    h = 0.5 / 13
+    for a in (x, y, z):
+        a = a.numpy()
+        assert a.dtype == np.float32 and np.all(np.abs(a) <= h)
+    counts = np.diff(cs)
+    assert counts.max() > 5 * counts.mean()  # clumps
+    x2, _, _, cs2 = synth.clustered_box_device(60000, 13, seed=4, device="cpu", chunk=1 << 14)
+    assert np.array_equal(cs, cs2) and np.array_equal(x.numpy(), x2.numpy())
