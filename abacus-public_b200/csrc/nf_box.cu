@@ -1360,17 +1360,8 @@ static nf_status new_plan(nf_ctx *ctx, nf_box *box, int lo, int hi, int variant,
 
 // Device time of one launch of a plan's pencil kernel (no co-add).
 static nf_status time_pencil(nf_ctx *ctx, nf_box *box, Plan &pl, float *ms) {
-    cudaStream_t st = ctx->stream;
-    KParams kp = make_params(ctx, box, pl);
-    KernelFn fn = pick_kernel(ctx->cfg.softening, ctx->cfg.b2 > 0.f, pl.variant);
-    NF_CUDA(cudaMemsetAsync(pl.d_counters, 0, 2 * sizeof(int), st));
-    NF_CUDA(cudaEventRecord(ctx->ev[0], st));
-    if (pl.n_heavy_groups + pl.n_light > 0) {
-        void *args[] = {&kp};
-        NF_CUDA(cudaLaunchKernel((const void *)fn, dim3(pl.grid), dim3(WARPS_PER_CTA * 32), args,
-                                 kernel_smem(), st));
-    }
-    NF_CUDA(cudaEventRecord(ctx->ev[1], st));
+    nf_status st = enqueue_pencil(ctx, box, pl, ctx->stream, cudaEventRecordDefault);
+    if (st != NF_OK) return st;
     NF_CUDA(cudaEventSynchronize(ctx->ev[1]));
     NF_CUDA(cudaEventElapsedTime(ms, ctx->ev[0], ctx->ev[1]));
     return NF_OK;
