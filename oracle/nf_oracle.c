@@ -19,7 +19,7 @@
  *     reproduces the reference compiled the same way bit for bit.
  *
  *  2. nfo_fp64_sinks(): an FP64 direct sum over the identical 5x5x5 cell
- *     neighbourhoods (the precision judge).  Global positions are
+ *     neighbourhoods (the precision yardstick).  Global positions are
  *     (double)float32 local position + (double) cell offset; the softening
  *     formulas are the reference's, evaluated in double.
  *
@@ -254,7 +254,7 @@ static inline double k64(int soft, double r2, double eps) {
 
 /* FP64 acceleration of the listed sink particles (global indices), summed
  * over the 5x5x5 cells around each sink's cell.  eps as for the FP32 path
- * (pass (double) of the float value to judge exactly that function). */
+ * (pass (double) of the float value to measure exactly that function). */
 int nfo_fp64_sinks(int cpd, int R, const int64_t *cell_start, const float *x, const float *y,
                    const float *z, int soft, double eps, const int64_t *sinks, int64_t nsinks,
                    double *acc) {
