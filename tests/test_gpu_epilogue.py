@@ -89,3 +89,26 @@ def test_pipelined_step_equals_chunked_sweeps(capi, synth, kbox, chunks):
         with pytest.raises(capi.NfError):
             db.step(x, y, z, out, kbox.cpd)  # chunks of fewer than R slabs
         db.close()
+
+
+def test_new_entry_points_reject_bad_arguments(capi, synth, kbox):
+    import ctypes
+    lib = capi.lib()
+    eps = synth.kernel_eps(1, synth.plummer_eps(41))
+    with capi.Context(softening=1, eps=eps) as ctx:
+        db = ctx.box(kbox)
+        k = capi.KickParams(1.0, 1.0, 0.0, 0.0, 0.0)
+        vel = np.zeros((kbox.n, 3), np.float32)
+        assert lib.nf_box_kick(ctx.h, db.h, 0, kbox.cpd, ctypes.byref(k), None, None, None,
+                               None) == capi.NF_EINVAL                      # no velocities
+        assert lib.nf_box_kick(ctx.h, db.h, 3, 3, ctypes.byref(k), None, vel.ctypes.data, None,
+                               None) == capi.NF_EINVAL                      # empty range
+        assert lib.nf_box_kick(ctx.h, db.h, 0, kbox.cpd + 1, ctypes.byref(k), None,
+                               vel.ctypes.data, None, None) == capi.NF_EINVAL
+        assert lib.nf_box_update_aos(ctx.h, db.h, None) == capi.NF_EINVAL
+        out = np.zeros((kbox.n, 4), np.float32)
+        assert lib.nf_box_step(ctx.h, db.h, None, None, None, out.ctypes.data, 0) == capi.NF_EINVAL
+        # still usable afterwards
+        a = db.forces(0, 1)
+        assert np.all(np.isfinite(a))
+        db.close()
