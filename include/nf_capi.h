@@ -287,7 +287,10 @@ nf_status nf_driver_plan_sic(nf_driver *drv, int slab, int jlow, int jhigh, nf_s
 nf_status nf_box_create(nf_ctx *ctx, int cpd, int64_t np, const int64_t *cell_start,
                         const float *x, const float *y, const float *z, nf_box **out);
 /* Replace the positions of a registered box (same cell counts); x, y, z
- * may be host or device arrays (CUDA unified addressing). */
+ * may be host or device arrays (CUDA unified addressing).  Calls on one
+ * context are serialised, but a serving request of the box that is still
+ * running reads the positions being replaced: update a box only between
+ * its requests (nf_server_wait). */
 nf_status nf_box_update(nf_ctx *ctx, nf_box *box, const float *x, const float *y,
                         const float *z);
 void nf_box_destroy(nf_ctx *ctx, nf_box *box);
