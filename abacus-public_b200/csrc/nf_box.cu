@@ -787,9 +787,10 @@ static nf_status build_plan(nf_ctx *ctx, nf_box *box, int lo, int hi, int varian
                     int S;
                     if (forced_S)
                         S = std::min(forced_S, smax);
-                    else
+                    else  // smallest tile that holds the rest; a rest of 65-96 sinks
+                          // takes 64 + 32 slots instead of 128
                         S = rem <= 32 ? 1
-                            : (rem <= 64 || smax == 2) ? 2
+                            : (rem <= 96 || smax == 2) ? 2
                             : (rem <= 128 || smax == 4) ? 4 : 8;
                     int take = (int)std::min<int64_t>(rem, 32 * S);
                     HostTile t;
