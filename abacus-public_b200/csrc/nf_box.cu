@@ -1487,6 +1487,17 @@ extern "C" nf_status nf_box_kick(nf_ctx *ctx, nf_box *box, int lo, int hi,
     }
     std::lock_guard<std::mutex> lk(ctx->mu);
     NF_CUDA(cudaSetDevice(ctx->device));
+    // the kernel dereferences these directly: they must be device-accessible
+    for (const void *q : {(const void *)far_acc, (const void *)vel, (const void *)acc_out,
+                          (const void *)cell_stats}) {
+        if (!q) continue;
+        cudaPointerAttributes pa;
+        if (cudaPointerGetAttributes(&pa, q) != cudaSuccess || !pa.devicePointer) {
+            cudaGetLastError();
+            set_error("nf_box_kick: far_acc, vel, acc_out and cell_stats must be device memory");
+            return NF_EINVAL;
+        }
+    }
     Plan *pl = nullptr;
     nf_status st = get_plan(ctx, box, lo, hi, &pl);
     if (st != NF_OK) return st;
