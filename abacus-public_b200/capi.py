@@ -70,7 +70,8 @@ class SicDesc(ctypes.Structure):
                 ("sink_nslab", ctypes.c_uint64), ("source_pos_slab", ctypes.c_void_p),
                 ("source_nslab", ctypes.c_void_p), ("sink_acc_slab", ctypes.c_void_p),
                 ("b2", ctypes.c_float), ("bytes_to_device", ctypes.c_void_p),
-                ("bytes_from_device", ctypes.c_void_p)]
+                ("bytes_from_device", ctypes.c_void_p), ("node_z_start", ctypes.c_int),
+                ("node_z_size", ctypes.c_int)]
 
 
 CELLINFO_DTYPE = np.dtype([("startindex", "<u8"), ("startindex_with_ghost", "<u8"),
@@ -90,7 +91,8 @@ class DriverParams(ctypes.Structure):
                 ("softening_length", ctypes.c_double), ("density_kernel_rad2", ctypes.c_float),
                 ("direct_bpd", ctypes.c_int), ("mem_per_gpu_buffer_gb", ctypes.c_double),
                 ("max_ram_mb", ctypes.c_double), ("use_pinned_gpu_memory", ctypes.c_int),
-                ("accumulation", ctypes.c_int), ("out_kind", ctypes.c_int)]
+                ("accumulation", ctypes.c_int), ("out_kind", ctypes.c_int),
+                ("node_z_start", ctypes.c_int), ("node_z_size", ctypes.c_int)]
 
 
 class DriverStats(ctypes.Structure):
@@ -447,24 +449,81 @@ class AbacusSlabs:
         return out
 
 
+class AbacusNodeSlabs:
+    """One node of a 2D (x, z) split as abacus holds it: the node owns z cells
+    [zs, zs + zn) of every slab; PosXYZ holds, row by row, the R ghost cells
+    below, the primary cells and the R ghost cells above
+    (startindex_with_ghost), AccSlab the primary cells only (startindex);
+    cells outside [zs - R, zs + zn + R) are empty.  `mask` marks the
+    particles whose accelerations this node produces."""
+
+    def __init__(self, box, zs: int, zn: int, R: int = 2, record_width: int = 4):
+        cpd = self.cpd = box.cpd
+        c2 = cpd * cpd
+        zcells = [(zs + dz) % cpd for dz in range(-R, zn + R)]
+        self.posxyz, self.cellinfo, self.acc, self.maps, self.nslab = [], [], [], [], []
+        self.mask = np.zeros(box.n, bool)
+        for s in range(cpd):
+            ci = np.zeros(c2, dtype=CELLINFO_DTYPE)
+            pos, acc_map = [], []
+            ng = npri = 0
+            for y in range(cpd):
+                for i, z in enumerate(zcells):
+                    c = (s * cpd + y) * cpd + z
+                    a, b = int(box.cell_start[c]), int(box.cell_start[c + 1])
+                    ci[y * cpd + z]["startindex_with_ghost"] = ng
+                    ci[y * cpd + z]["startindex"] = npri
+                    ci[y * cpd + z]["count"] = b - a
+                    ci[y * cpd + z]["active"] = b - a
+                    pos.append(np.arange(a, b))
+                    ng += b - a
+                    if R <= i < R + zn:
+                        acc_map.append(np.arange(a, b))
+                        npri += b - a
+            idx = np.concatenate(pos) if pos else np.zeros(0, np.int64)
+            amap = np.concatenate(acc_map) if acc_map else np.zeros(0, np.int64)
+            self.mask[amap] = True
+            self.posxyz.append(np.ascontiguousarray(
+                np.concatenate([box.x[idx], box.y[idx], box.z[idx]]), dtype=np.float32))
+            self.nslab.append(len(idx))
+            self.cellinfo.append(ci)
+            self.maps.append(amap)
+            self.acc.append(np.zeros((max(len(amap), 1), record_width), dtype=np.float32))
+
+    def view(self, s: int) -> SlabView:
+        return SlabView(self.posxyz[s].ctypes.data, self.nslab[s], self.cellinfo[s].ctypes.data,
+                        self.acc[s].ctypes.data)
+
+    def gather_acc(self, n: int) -> np.ndarray:
+        out = np.zeros((n, self.acc[0].shape[1]), dtype=np.float32)
+        for m, a in zip(self.maps, self.acc):
+            out[m] = a[:len(m)]
+        return out
+
+
 class Driver:
-    """nf_driver: the NearFieldDriver mirror (device < 0: planner only)."""
+    """nf_driver: the NearFieldDriver mirror (device < 0: planner only).
+    node_z = (node_z_start, node_z_size) runs one node of a 2D z-split."""
 
     def __init__(self, box, softening: int, softening_length: float, device: int = 0,
                  near_field_radius: int = 2, direct_bpd: int = 3, mem_gb: float = 0.0,
                  b2: float = 0.0, accumulation: int = ACC_COMPENSATED,
-                 out_kind: int = OUT_FLOAT4, use_pinned: int = -1):
+                 out_kind: int = OUT_FLOAT4, use_pinned: int = -1,
+                 node_z: tuple[int, int] | None = None):
+        zs, zn = node_z if node_z else (0, 0)
         p = DriverParams(device=device, cpd=box.cpd, np=box.n,
                          near_field_radius=near_field_radius, softening=softening,
                          softening_length=softening_length, density_kernel_rad2=b2,
                          direct_bpd=direct_bpd, mem_per_gpu_buffer_gb=mem_gb, max_ram_mb=0.0,
                          use_pinned_gpu_memory=use_pinned, accumulation=accumulation,
-                         out_kind=out_kind)
+                         out_kind=out_kind, node_z_start=zs, node_z_size=zn)
         h = ctypes.c_void_p()
         check(lib().nf_driver_create(ctypes.byref(p), ctypes.byref(h)), "nf_driver_create")
         self.h = h
         self.box = box
-        self.slabs = AbacusSlabs(box, 4 if out_kind == OUT_FLOAT4 else 3)
+        rw = 4 if out_kind == OUT_FLOAT4 else 3
+        self.slabs = (AbacusNodeSlabs(box, zs, zn, near_field_radius, rw) if zn
+                      else AbacusSlabs(box, rw))
         for s in range(box.cpd):
             v = self.slabs.view(s)
             check(lib().nf_driver_set_slab(self.h, s, ctypes.byref(v)), "nf_driver_set_slab")

@@ -8,9 +8,10 @@
 // singletons (CP cell info, SB slab buffers, SS slab sizes, P parameters);
 // here the caller registers one view per slab (nf_slab_view) and the driver
 // reads those.  Differences by design: no CPU fallback (ForceCPU and
-// CheckGPUCPU live in the test oracle, not in the product), no MPI 2D ghost
-// layout (one z-domain per node), SIC arrays owned by the SIC instead of a
-// slab arena.
+// CheckGPUCPU live in the test oracle, not in the product), SIC arrays owned
+// by the SIC instead of a slab arena.  The MPI 2D z-split is the
+// node_z_start / node_z_size pair of nf_driver_params (the reference's
+// globals of the same names).
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -47,7 +48,8 @@ struct STimer {
 
 // The caller's slabs (replaces CP / SB / SS lookups).
 struct SlabEnv {
-    int cpd = 0;
+    int cpd = 0, R = 2;
+    int zs = 0, zn = 0;  // 2D z-split node (zn = 0: one z-domain)
     std::vector<nf_slab_view> slabs;
     std::vector<char> present;
     int wrap(int i) const {
@@ -57,8 +59,15 @@ struct SlabEnv {
     const nf_cellinfo &cell(int x, int y, int z) const {
         return slabs[wrap(x)].cellinfo[(size_t)wrap(y) * cpd + wrap(z)];
     }
-    // NumParticlesInSkewer (PencilOnPencil.cc:90-109): particles of row j.
+    // NumParticlesInSkewer (PencilOnPencil.cc:90-109): particles of row j
+    // (2D: of the node's z range, ghost cells included for sources).
     uint64_t skewer(int slab, int j, bool ghost) const {
+        if (zn > 0) {
+            uint64_t n = 0;
+            const int pad = ghost ? R : 0;
+            for (int z = zs - pad; z < zs + zn + pad; z++) n += (uint64_t)cell(slab, j, z).count;
+            return n;
+        }
         const nf_slab_view &v = slabs[wrap(slab)];
         const nf_cellinfo &c0 = v.cellinfo[(size_t)j * cpd];
         uint64_t start = ghost ? c0.startindex_with_ghost : c0.startindex;
@@ -109,13 +118,16 @@ class SetInteractionCollection {
 
     int NumPaddedBlocks(int n) const { return (n + NFBlockSize - 1) / NFBlockSize; }
     int PaddedSinkCount(int i) const { return NFBlockSize * NumPaddedBlocks(SinkSetCount[i]); }
-    // index_to_zcen (PencilOnPencil.cc:37-43), one z-domain per node: the
-    // first pencil is the first whose cells all lie in the primary range.
+    // index_to_zcen (PencilOnPencil.cc:37-43): the first pencil is the
+    // first whose cells all lie in the primary range; 2D pencils also centre
+    // on the R ghost cells each side (no z wrap).
     int index_to_zcen(int k) const {
         int kk = k + k_low + nfradius;
-        if (kk >= k_low + (k_high - k_low)) kk -= (k_high - k_low);
+        const int pad = twoD ? nfradius : 0;
+        if (kk >= k_high + pad) kk -= (k_high - k_low) + 2 * pad;
         return kk;
     }
+    bool twoD = false;
 
   private:
     nf_sic_desc desc_{};
@@ -139,9 +151,11 @@ SetInteractionCollection::SetInteractionCollection(const SlabEnv &env, const nf_
     nfradius = NearFieldRadius;
     nfwidth = 2 * NearFieldRadius + 1;
     j_width = j_high - j_low;
-    k_low = 0;
-    k_high = cpd;
-    Nk = k_high - k_low;
+    // k_low, k_high: the node's primary sink cells (PencilOnPencil.cc:200-204)
+    twoD = env.zn > 0;
+    k_low = twoD ? env.zs : 0;
+    k_high = twoD ? env.zs + env.zn : cpd;
+    Nk = twoD ? k_high - k_low + nfwidth - 1 : k_high - k_low;
     const int W = nfwidth;
     if ((uint64_t)j_width * Nk >= INT32_MAX) {
         fail("NSinkSets would overflow int32");
@@ -163,8 +177,9 @@ SetInteractionCollection::SetInteractionCollection(const SlabEnv &env, const nf_
     SourceSetCount.assign(NSourceSets, 0);
     SourcePlan.assign((size_t)NSourceSets * W, nf_cell_plan{0, 0});
 
-    // Sink pencils: cells (slab, y, zc-R .. zc+R); wrapcell = first cell whose
-    // wrapped z is 0 (SinkPencilPlan::load, PencilPlan.cc:95-138).
+    // Sink pencils: cells (slab, y, zc-R .. zc+R); wrapcell = the cell where
+    // z wraps or leaves the primary range; 2D pencils are truncated to the
+    // primary cells (SinkPencilPlan::load, PencilPlan.cc:95-138).
     std::vector<uint64_t> skewer_blocks(j_width + nfwidth, 0);
     for (int j = 0; j < j_width; j++)
         for (int k = 0; k < Nk; k++) {
@@ -173,10 +188,14 @@ SetInteractionCollection::SetInteractionCollection(const SlabEnv &env, const nf_
             int total = 0, wrapcell = 0;
             for (int c = 0; c < W; c++) {
                 int zc = zmid + c - nfradius;
-                const nf_cellinfo &ci = env.cell(slab, j + j_low, zc);
-                SinkPlan[(size_t)si * W + c] = nf_cell_plan{(uint32_t)ci.startindex, ci.count};
-                if (env.wrap(zc) == 0) wrapcell = c;
-                total += ci.count;
+                if (twoD && env.wrap(zc - k_low) >= k_high - k_low) {
+                    SinkPlan[(size_t)si * W + c] = nf_cell_plan{0, 0};  // no-op cell
+                } else {
+                    const nf_cellinfo &ci = env.cell(slab, j + j_low, zc);
+                    SinkPlan[(size_t)si * W + c] = nf_cell_plan{(uint32_t)ci.startindex, ci.count};
+                    total += ci.count;
+                }
+                if (env.wrap(zc - k_high) == 0 || env.wrap(zc) == k_low) wrapcell = c;
             }
             SinkWrapcell[si] = wrapcell;
             SinkSetCount[si] = total;
@@ -314,6 +333,8 @@ nf_status SetInteractionCollection::GPUExecute(nf_ctx *ctx, const SlabEnv &env, 
     d.b2 = b2;
     d.bytes_to_device = &bytes_to_device;
     d.bytes_from_device = &bytes_from_device;
+    d.node_z_start = twoD ? k_low : 0;
+    d.node_z_size = twoD ? k_high - k_low : 0;
     DeviceThreadTimer.Start();
     return nf_sic_execute(ctx, &d, j_low, j_high, blocking, &CompletionFlag);
 }
@@ -389,7 +410,17 @@ NearFieldDriver::NearFieldDriver(const nf_driver_params &p, nf_status *st) : par
         *st = NF_EINVAL;
         return;
     }
+    if (p.node_z_size < 0 || (p.node_z_size > 0 && (p.node_z_start < 0 || p.node_z_start >= p.cpd ||
+                                                      p.node_z_size + 2 * RADIUS > p.cpd))) {
+        nf::set_error("nf_driver_create: 2D node needs 0 <= node_z_start < cpd and "
+                      "node_z_size + 2R <= cpd");
+        *st = NF_EINVAL;
+        return;
+    }
     env.cpd = p.cpd;
+    env.R = RADIUS;
+    env.zs = p.node_z_size > 0 ? p.node_z_start : 0;
+    env.zn = p.node_z_size;
     env.slabs.assign(p.cpd, nf_slab_view{nullptr, 0, nullptr, nullptr});
     env.present.assign(p.cpd, 0);
     work_.resize(p.cpd);

@@ -175,9 +175,13 @@ static nf_status check_desc(nf_ctx *ctx, const nf_sic_desc &d, int jlow, int jhi
         set_error("nf_sic_execute: nfradius differs from the context's near_field_radius");
         return NF_EINVAL;
     }
-    if (d.cpd < W || (d.cpd & 1) == 0 || d.nk != d.cpd || jlow < 0 || jhigh > d.cpd ||
-        jlow >= jhigh) {
-        set_error("nf_sic_execute: bad geometry (odd cpd >= 2R+1, Nk == cpd, 0 <= jlow < jhigh <= cpd)");
+    const bool two_d = d.node_z_size > 0;
+    if (d.cpd < W || (d.cpd & 1) == 0 || jlow < 0 || jhigh > d.cpd || jlow >= jhigh ||
+        (!two_d && d.nk != d.cpd) ||
+        (two_d && (d.nk != d.node_z_size + 2 * R || d.node_z_size + 2 * R > d.cpd ||
+                   d.node_z_start < 0 || d.node_z_start >= d.cpd))) {
+        set_error("nf_sic_execute: bad geometry (odd cpd >= 2R+1, 0 <= jlow < jhigh <= cpd, Nk == "
+                  "cpd; 2D: Nk == node_z_size + 2R, node_z_size + 2R <= cpd)");
         return NF_EINVAL;
     }
     const int jw = jhigh - jlow;
@@ -212,10 +216,20 @@ static nf_status run_task(nf_ctx *ctx, SicBuffer &b, const SicTask &t) {
     const int jw = t.jhigh - t.jlow, nrows = jw + 2 * R;
     const int64_t ncell = (int64_t)W * cpd * cpd;
     // Pencil k of a row is centred on z = (k + R) mod cpd (index_to_zcen,
-    // PencilOnPencil.cc:37-43, one z-domain per node).
-    auto zcen = [&](int k) { return (k + R) % cpd; };
+    // PencilOnPencil.cc:37-43, one z-domain per node); 2D: on node_z_start +
+    // k + R, brought back by node_z_size + 2R past the upper ghost edge, so
+    // the centres cover the primary cells and R ghost cells on each side.
+    const bool two_d = d.node_z_size > 0;
+    const int zs = d.node_z_start, zn = d.node_z_size;
+    auto zcen = [&](int k) {
+        if (!two_d) return (k + R) % cpd;
+        int kk = k + zs + R;
+        if (kk >= zs + zn + R) kk -= zn + 2 * R;
+        return wrapi(kk, cpd);
+    };
+    auto primary = [&](int z) { return !two_d || wrapi(z - zs, cpd) < zn; };
     // cell counts of the mini box: slot s = source slab x-R+s, rows of the SIC
-    std::vector<int64_t> cnt(ncell, 0), rowstart(W * cpd, -1);
+    std::vector<int64_t> cnt(ncell, 0), rowstart(W * cpd, -1), cellstart(two_d ? ncell : 0, -1);
     std::vector<char> row_used(cpd, 0);
     for (int r = 0; r < nrows; r++) {
         int y = wrapi(t.jlow - R + r, cpd);
@@ -229,7 +243,8 @@ static nf_status run_task(nf_ctx *ctx, SicBuffer &b, const SicTask &t) {
                     return NF_EINVAL;
                 }
                 cnt[((int64_t)s * cpd + y) * cpd + z] = pl[s].n;
-                if (z == 0) rowstart[s * cpd + y] = pl[s].start;
+                if (two_d) cellstart[((int64_t)s * cpd + y) * cpd + z] = pl[s].start;
+                else if (z == 0) rowstart[s * cpd + y] = pl[s].start;
             }
         }
     }
@@ -251,8 +266,20 @@ static nf_status run_task(nf_ctx *ctx, SicBuffer &b, const SicTask &t) {
     for (int j = 0; j < jw; j++)
         for (int k = 0; k < nk; k++) {
             int y = t.jlow + j, zc = zcen(k);
-            int64_t np_ = 0;
-            for (int a = -R; a <= R; a++) np_ += count(R, y, zc + a);
+            // 2D: the primary cells of a pencil are contiguous in its sink
+            // stream, after g_lo ghost sinks; only they are swept (the
+            // reference truncates sink pencils the same way,
+            // PencilPlan.cc:110-116)
+            int64_t np_ = 0, g_lo = 0;
+            bool seen_primary = false;
+            for (int a = -R; a <= R; a++) {
+                if (primary(zc + a)) {
+                    np_ += count(R, y, zc + a);
+                    seen_primary = true;
+                } else if (!seen_primary) {
+                    g_lo += count(R, y, zc + a);
+                }
+            }
             if (np_ != d.sink_set_count[j * nk + k]) {
                 set_error("nf_sic_execute: SinkSetCount disagrees with the source plans");
                 return NF_EINVAL;
@@ -264,7 +291,8 @@ static nf_status run_task(nf_ctx *ctx, SicBuffer &b, const SicTask &t) {
             int pencil = (int)(((int64_t)R * cpd + y) * cpd + zc);
             for (int64_t b0 = 0; b0 < np_; b0 += NFBLOCK) {
                 int take = (int)std::min<int64_t>(NFBLOCK, np_ - b0);
-                items.push_back(Item{pencil, (int)b0, take, take <= 32 ? 1 : 2, 0, (int)M, 0, 0});
+                items.push_back(
+                    Item{pencil, (int)(g_lo + b0), take, take <= 32 ? 1 : 2, 0, (int)M, 0, 0});
             }
         }
     nitems = items.size();
@@ -275,7 +303,22 @@ static nf_status run_task(nf_ctx *ctx, SicBuffer &b, const SicTask &t) {
     for (int s = 0; s < W; s++) {
         const float *slab = d.source_pos_slab[s];
         const uint64_t ns = d.source_nslab[s];
-        for (int y = 0; y < cpd; y++) {
+        for (int y = 0; y < cpd && two_d; y++) {  // 2D: cell by cell (ghost cells included)
+            if (!row_used[y]) continue;
+            for (int z = 0; z < cpd; z++) {
+                const int64_t c = ((int64_t)s * cpd + y) * cpd + z;
+                const int64_t n = cnt[c], src = cellstart[c], dst = cs[c];
+                if (n == 0) continue;
+                if (src < 0 || (uint64_t)(src + n) > ns) {
+                    set_error("nf_sic_execute: source cell outside its slab");
+                    return NF_EINVAL;
+                }
+                memcpy(hx + dst, slab + src, n * sizeof(float));
+                memcpy(hy + dst, slab + ns + src, n * sizeof(float));
+                memcpy(hz + dst, slab + 2 * ns + src, n * sizeof(float));
+            }
+        }
+        for (int y = 0; y < cpd && !two_d; y++) {
             if (!row_used[y]) continue;
             int64_t dst = cs[((int64_t)s * cpd + y) * cpd];
             int64_t n = cs[((int64_t)s * cpd + y + 1) * cpd] - dst;
@@ -321,8 +364,25 @@ static nf_status run_task(nf_ctx *ctx, SicBuffer &b, const SicTask &t) {
     const size_t rec = ctx->cfg.out_kind == NF_OUT_FLOAT4 ? 16 : 12;
     NF_CUDA(cudaMemcpyAsync(b.h_out, b.d_out, (size_t)n_sinks * rec, cudaMemcpyDeviceToHost, sm));
     NF_CUDA(cudaStreamSynchronize(sm));
-    // AccSlab rows [jlow, jhigh) are contiguous from the first sink cell of row jlow
-    if (n_sinks > 0) {
+    if (two_d) {
+        // primary cells only, each at its AccSlab start (the centre cell of
+        // the pencil centred on it)
+        for (int j = 0; j < jw; j++)
+            for (int k = 0; k < nk; k++) {
+                const int y = t.jlow + j, zc = zcen(k);
+                if (!primary(zc)) continue;
+                const nf_cell_plan &ce = d.sink_plan[((int64_t)j * nk + k) * W + R];
+                const int64_t c = ((int64_t)R * cpd + y) * cpd + zc;
+                if (ce.n != cnt[c]) {
+                    set_error("nf_sic_execute: sink plan and source plan disagree on a cell");
+                    return NF_EINVAL;
+                }
+                if (ce.n)
+                    memcpy((char *)d.sink_acc_slab + (size_t)ce.start * rec,
+                           (char *)b.h_out + (size_t)(cs[c] - p0) * rec, (size_t)ce.n * rec);
+            }
+    } else if (n_sinks > 0) {
+        // AccSlab rows [jlow, jhigh) are contiguous from the first sink cell of row jlow
         // the centre cell of the row-jlow pencil centred on z = 0 is cell (jlow, 0)
         int k0 = (cpd - R) % cpd;
         int64_t acc0 = d.sink_plan[(int64_t)k0 * W + R].start;

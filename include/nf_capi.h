@@ -168,6 +168,15 @@ typedef struct nf_sic_desc {
     float b2;
     /* counters written back (SetInteractionCollection.hh:182-183, 243-248) */
     uint64_t *bytes_to_device, *bytes_from_device;
+    /* 2D z-split layout (MPI_size_z > 1; PencilOnPencil.cc:37-43, 200-204,
+     * PencilPlan.cc:95-138): this node's primary z cells are
+     * [node_z_start, node_z_start + node_z_size); Nk = node_z_size + 2R
+     * pencils centred from node_z_start - R (index_to_zcen with pad R, no z
+     * wrap); sink plans truncated to primary cells with AccSlab starts
+     * (startindex), source plans with PosXYZ starts including ghost cells
+     * (startindex_with_ghost).  node_z_size = 0: the whole z range (Nk = cpd).
+     * Requires node_z_size + 2R <= cpd. */
+    int node_z_start, node_z_size;
 } nf_sic_desc;
 
 /* Run one SIC (GPUPencilTask): gather pencils, H2D, kernel, D2H, co-add
@@ -222,6 +231,13 @@ typedef struct nf_driver_params {
     int use_pinned_gpu_memory;     /* P.UsePinnedGPUMemory (-1 = auto) */
     int accumulation;              /* NF_ACC_* */
     int out_kind;                  /* NF_OUT_* (accstruct) */
+    /* 2D z-split (MPI_size_z > 1): this node's primary z cells
+     * [node_z_start, node_z_start + node_z_size) (node_z_size = 0: all of z).
+     * Slab views then only need the cells z in [node_z_start - R,
+     * node_z_start + node_z_size + R) filled: startindex numbers primary
+     * cells (AccSlab), startindex_with_ghost numbers PosXYZ (ghosts too).
+     * Requires node_z_size + 2R <= cpd. */
+    int node_z_start, node_z_size;
 } nf_driver_params;
 
 /* NearFieldDriver statistics (directdriver.cpp:41-77, filled by Finalize and
