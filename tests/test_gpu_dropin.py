@@ -24,8 +24,7 @@ def _check(oracle, box, soft, eps, a):
     assert rms <= 2e-6 and mx <= 1e-4, (rms, mx)
 
 
-@pytest.mark.parametrize("soft", [0, 1])
-@pytest.mark.parametrize("blocking", [0, 1])
+@pytest.mark.parametrize("soft,blocking", [(0, 0), (0, 1), (1, 0), (1, 1), (2, 0), (3, 1)])
 def test_driver_matches_oracle(capi, oracle, synth, soft, blocking):
     box = synth.clustered_box(50000, 13, seed=41, n_clumps=30)
     length = synth.plummer_eps(37)
@@ -100,9 +99,10 @@ def test_driver_errors(capi, synth):
         drv.close()
 
 
-@pytest.mark.parametrize("soft,nodes", [(0, [(0, 5), (5, 4), (9, 4)]),
-                                        (1, [(11, 5), (3, 4), (7, 4)])])
-def test_driver_2d_z_split(capi, oracle, synth, soft, nodes):
+@pytest.mark.parametrize("soft,nodes,out_kind", [(0, [(0, 5), (5, 4), (9, 4)], 0),
+                                                 (1, [(11, 5), (3, 4), (7, 4)], 0),
+                                                 (2, [(2, 7), (9, 6)], 1)])
+def test_driver_2d_z_split(capi, oracle, synth, soft, nodes, out_kind):
     """A 2D (x, z) split: each node runs the drop-in on its own z cells plus
     R ghost cells each side (MPI_size_z > 1 layout) and produces its primary
     particles; the nodes together match the one-domain drop-in and the
@@ -110,11 +110,12 @@ def test_driver_2d_z_split(capi, oracle, synth, soft, nodes):
     box = synth.clustered_box(50000, 13, seed=44, n_clumps=30)
     length = synth.plummer_eps(37)
     eps = synth.kernel_eps(soft, length)
-    a2 = np.zeros((box.n, 4), np.float32)
+    ok_kind = capi.OUT_FLOAT4 if out_kind == 0 else capi.OUT_FLOAT3
+    a2 = np.zeros((box.n, 4 if out_kind == 0 else 3), np.float32)
     covered = np.zeros(box.n, int)
     for zs, zn in nodes:
         drv = capi.Driver(box, softening=soft, softening_length=length, direct_bpd=2,
-                          node_z=(zs, zn))
+                          node_z=(zs, zn), out_kind=ok_kind)
         try:
             a = drv.run_all()
             assert drv.stats().direct_interactions > 0
@@ -124,7 +125,8 @@ def test_driver_2d_z_split(capi, oracle, synth, soft, nodes):
         a2[m] = a[m]
         covered += m
     assert np.all(covered == 1)
-    drv = capi.Driver(box, softening=soft, softening_length=length, direct_bpd=2)
+    drv = capi.Driver(box, softening=soft, softening_length=length, direct_bpd=2,
+                      out_kind=ok_kind)
     try:
         a1 = drv.run_all()
     finally:
