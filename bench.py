@@ -76,6 +76,31 @@ def make_box(w, seed_offset=0):
     return synth.clustered_box(n, w["cpd"], w["seed"] + seed_offset)
 
 
+def box_nc(w):
+    """Partial components per sink: x, y, z (+ density when b2 > 0)."""
+    return 4 if w.get("b2", 0.0) > 0 else 3
+
+
+def staging_hbm(n, nc, kernel_ms, traffic, R=2):
+    """HBM side of the pencil kernel: algorithmic bytes per launch (one
+    16-byte position record per particle read, (2R+1) x nc double partials per
+    particle written), the rate they imply over the launch, and the same for
+    the ncu-measured DRAM bytes when a capture is on file."""
+    alg = n * (16 + (2 * R + 1) * nc * 8)
+    secs = kernel_ms / 1e3
+    out = {"algorithmic_bytes": int(alg), "algorithmic_gbs": alg / secs / 1e9,
+           "measured_bytes": traffic,
+           "measured_gbs": None if traffic is None else traffic / secs / 1e9}
+    peaks = ROOT / "MEASURED_PEAKS.json"
+    try:
+        hbm = float(json.loads(peaks.read_text())["hbm_gbs"])
+        out["hbm_peak_gbs"] = hbm
+        out["frac_of_hbm_peak"] = out["algorithmic_gbs"] / hbm
+    except (OSError, ValueError, KeyError):
+        pass
+    return out
+
+
 def kernel_eps(w):
     from abacus_public_b200 import synth
     return synth.kernel_eps(w["softening"], synth.plummer_eps(w["n_side"]))
@@ -579,7 +604,8 @@ def our_arm(args, w):
                      "flops_per_pair": flops,
                      "peak_source": "FFMA microbenchmark on this GPU in this run, sustained "
                                     "(MEASURED_PEAKS.json has no FP32 figure)",
-                     "peak_burst": peak_burst},
+                     "peak_burst": peak_burst,
+                     "staging_hbm": staging_hbm(n, box_nc(w), k_ms, traffic)},
         "e2e": {"value": e2e_value, "unit": "pairs/s", "ms_per_step": e2e_ms,
                 "h2d_bytes_per_step": int(12 * n), "d2h_bytes_per_step": int(16 * n)},
         "gpu_launches": int(launches),
@@ -673,7 +699,8 @@ def big_arm(args, w):
                    "max_particles_per_cell": int(counts.max()), "kernel_shape": 0},
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak_s, "unit": "TFLOP/s",
                      "frac": achieved / peak_s, "traffic": None, "kernel": "pencil_kernel",
-                     "kernel_ms": k_ms, "flops_per_pair": flops},
+                     "kernel_ms": k_ms, "flops_per_pair": flops,
+                     "staging_hbm": staging_hbm(p1 - p0, box_nc(w), k_ms, None)},
         "accuracy_vs_fp64": {"rms_frac": rms, "max_frac": mx, "sinks": 2000},
         "gpu_launches": int(args.steps * t.launches),
         "clocks": clk.summary(),
@@ -742,7 +769,8 @@ def big_full_sweep(args, w, capi, ctx, db, hbox, eps, peak_s, stream):
         "roofline": {"bound": "fp32", "achieved": c["pairs"] * flops / (c["kernel_ms"] / 1e3) / 1e12,
                      "peak": peak_s, "unit": "TFLOP/s", "frac": c["frac_of_fp32_peak"],
                      "traffic": None, "kernel": "pencil_kernel", "kernel_ms": c["kernel_ms"],
-                     "flops_per_pair": flops},
+                     "flops_per_pair": flops,
+                     "staging_hbm": staging_hbm(hbox.n, box_nc(w), c["kernel_ms"], None)},
         "modes": modes,
         "accuracy_vs_fp64": {"rms_frac": c["rms_frac"], "max_frac": c["max_frac"], "sinks": 2000},
         "gpu_launches": 2 * len(ranges) * 2,
