@@ -86,3 +86,54 @@ def test_lattice_cancels(capi, synth):
             db.close()
         one = (1.0 / cpd) ** -2 if soft == 0 else (1.0 / cpd) ** -2 * float(eps) ** -1.5
         assert np.abs(a).max() < 1e-6 * one, (soft, float(np.abs(a).max()), one)
+
+
+@pytest.mark.parametrize("soft", [0, 1])
+def test_cell_faces_and_periodic_corner(capi, oracle, synth, soft):
+    """Particles exactly on cell faces (cell-relative -h/2, one ulp inside
+    either face, and 0 on each axis: 64 per cell) in the periodic corner
+    cell (0,0,0), an interior cell and a cell on the x = cpd-1 face, over a
+    random background.  The three face cells are not neighbours of each other,
+    so no two particles sit an ulp apart across a face, where any two FP32
+    implementations round the cell shift differently; inside a cell the
+    separations are exact.  Checked against the reference CPU restatement
+    (per component 1e-4 |a|) and the FP64 oracle (RMS 2e-6, max 1e-4)."""
+    cpd = 7
+    h = 1.0 / cpd
+    rng = np.random.default_rng(71)
+    n_bg = 3000
+    gpos = rng.random((n_bg, 3))
+    cell = np.floor(gpos * cpd).astype(np.int64) % cpd
+    local = (gpos - (cell + 0.5) * h).astype(np.float32)
+    lo = np.float32(-0.5 * h)
+    vals = np.array([lo, np.nextafter(lo, np.float32(1)),
+                     np.nextafter(np.float32(0.5 * h), np.float32(0)), np.float32(0)], np.float32)
+    face = np.array(np.meshgrid(vals, vals, vals, indexing="ij")).reshape(3, -1).T
+    cells, locs = [cell], [local]
+    for c in [(0, 0, 0), (3, 3, 3), (6, 3, 0)]:
+        cells.append(np.tile(np.array(c, np.int64), (len(face), 1)))
+        locs.append(face)
+    cell = np.concatenate(cells)
+    local = np.concatenate(locs)
+    cid = (cell[:, 0] * cpd + cell[:, 1]) * cpd + cell[:, 2]
+    order = np.argsort(cid, kind="stable")
+    cid, local = cid[order], local[order]
+    cs = np.zeros(cpd ** 3 + 1, np.int64)
+    np.cumsum(np.bincount(cid, minlength=cpd ** 3), out=cs[1:])
+    box = synth.Box(cpd=cpd, x=local[:, 0].copy(), y=local[:, 1].copy(), z=local[:, 2].copy(),
+                    cell_start=cs)
+    eps = synth.kernel_eps(soft, 0.05 * h)
+    with capi.Context(softening=soft, eps=eps) as ctx:
+        db = ctx.box(box)
+        a = db.forces()[:, :3].astype(np.float64)
+        db.close()
+    assert np.all(np.isfinite(a))
+    ref = np.zeros((box.n, 3), np.float32)
+    for s in range(cpd):
+        oracle.ref32_slab(box, soft, eps, s, acc=ref)
+    norm = np.linalg.norm(ref.astype(np.float64), axis=1)
+    assert np.all(norm > 0)
+    diff = np.abs(a - ref)
+    assert np.all(diff <= 1e-4 * norm[:, None]), float((diff / norm[:, None]).max())
+    rms, mx, _ = oracle.frac_errors(a, oracle.fp64_sinks(box, soft, eps, np.arange(box.n)))
+    assert rms <= 2e-6 and mx <= 1e-4, (rms, mx)
