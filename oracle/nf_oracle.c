@@ -28,6 +28,14 @@
  *     step, per-column FP32 partials folded into a compensated (hi, lo) sum).
  *     It lets the error budget of that arithmetic be studied on the CPU.
  *
+ *  4. nfo_cpu_execute(): SetInteractionCollection::CPUExecute
+ *     (singlestep/Direct/extras_PencilOnPencil.cc:7-152), the reference's CPU
+ *     twin of the GPU pencil kernel (Plummer only, as there): every padded
+ *     sink slot of every 64-sink block against the 2R+1 source pencils of its
+ *     interaction list, y offset added per interaction, FP32 throughout.  It
+ *     runs on the SIC arrays oracle.py builds in the reference's layout, so it
+ *     pins the pencil decomposition itself against the cell-loop direct.
+ *
  * Data layout (shared with the product library): a periodic unit box of
  * cpd^3 cells (cpd odd), particles sorted by cell id ((cx*cpd)+cy)*cpd+cz,
  * positions as three float32 arrays relative to the cell centre,
@@ -518,6 +526,53 @@ int nfo_fp64_density(int cpd, int R, const int64_t *cell_start, const float *x, 
                     }
                 }
         w[n] = acc;
+    }
+    return 0;
+}
+
+/* SetInteractionCollection::CPUExecute (extras_PencilOnPencil.cc:7-152).
+ * sink_xyz: X | Y | Z of nslots padded sink slots (z already shifted by
+ * (c-R) h per sink cell, PencilPlan.cc:22-90); src_xyz: X | Y | Z of nsrc
+ * sources (x shifted by (c-R) h per source cell, PencilPlan.cc:214-255);
+ * id_max[p]: one past the last live slot of sink pencil p; parent[b]: the
+ * pencil of block b; ilist / yoff: W source pencils and y offsets per sink
+ * pencil; eps2 = eps_int^2 (cpu_eps).  acc: 3 floats per slot, written for
+ * live slots only (extras_PencilOnPencil.cc:123-133). */
+int nfo_cpu_execute(int nblocks, int nslots, const float *sink_xyz, const uint32_t *id_max,
+                    const int32_t *parent, int nsrc, const float *src_xyz,
+                    const int32_t *src_start, const int32_t *src_count, const int32_t *ilist,
+                    const float *yoff, int W, float eps2, float *acc) {
+    if (nblocks < 0 || nslots < 64 * nblocks || W < 1) return -1;
+    const float *SX = sink_xyz, *SY = sink_xyz + nslots, *SZ = sink_xyz + 2 * (size_t)nslots;
+    const float *TX = src_xyz, *TY = src_xyz + nsrc, *TZ = src_xyz + 2 * (size_t)nsrc;
+    for (int b = 0; b < nblocks; b++) {
+        const int p = parent[b];
+        for (int t = 0; t < 64; t++) {
+            const int64_t id = 64 * (int64_t)b + t;
+            if (id >= (int64_t)id_max[p]) continue; /* padded slot: nothing stored */
+            const float sinkX = SX[id], sinkY = SY[id], sinkZ = SZ[id];
+            float ax = 0.f, ay = 0.f, az = 0.f;
+            for (int c = p * W; c < p * W + W; c++) {
+                const int s = ilist[c];
+                const int st = src_start[s], n = src_count[s];
+                const float yoffset = yoff[c];
+                if (st < 0 || n < 0 || (int64_t)st + n > nsrc) return -2;
+                for (int i = 0; i < n; i++) {
+                    float drx = TX[st + i] - sinkX;
+                    float dry = TY[st + i] - sinkY + yoffset;
+                    float drz = TZ[st + i] - sinkZ;
+                    /* (FLOAT)1./std::sqrt(float): the float overload */
+                    float r = 1.0f / sqrtf(drx * drx + dry * dry + drz * drz + eps2);
+                    r *= r * r;
+                    ax -= r * drx;
+                    ay -= r * dry;
+                    az -= r * drz;
+                }
+            }
+            acc[3 * id] = ax;
+            acc[3 * id + 1] = ay;
+            acc[3 * id + 2] = az;
+        }
     }
     return 0;
 }

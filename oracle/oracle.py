@@ -13,6 +13,7 @@ from __future__ import annotations
 import ctypes
 import os
 import pathlib
+from types import SimpleNamespace
 
 import numpy as np
 
@@ -24,6 +25,7 @@ SOFTENING_NAMES = {0: "plummer", 1: "single_spline", 2: "cubic_spline", 3: "cubi
 _i64p = np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")
 _f32p = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
 _f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
 
 _lib = None
 _ref = {}
@@ -47,6 +49,11 @@ def lib():
         L.nfo_fp64_density.argtypes = [ctypes.c_int, ctypes.c_int, _i64p, _f32p, _f32p, _f32p,
                                        ctypes.c_double, _i64p, ctypes.c_int64, _f64p]
         L.nfo_fp64_density.restype = ctypes.c_int
+        L.nfo_cpu_execute.argtypes = [ctypes.c_int, ctypes.c_int, _f32p,
+                                      np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS"),
+                                      _i32p, ctypes.c_int, _f32p, _i32p, _i32p, _i32p, _f32p,
+                                      ctypes.c_int, ctypes.c_float, _f32p]
+        L.nfo_cpu_execute.restype = ctypes.c_int
         L.nfo_pair_count.argtypes = [ctypes.c_int, ctypes.c_int, _i64p]
         L.nfo_pair_count.restype = ctypes.c_uint64
         for f in (L.nfo_ref32_slab, L.nfo_ref32_cells, L.nfo_fp64_sinks, L.nfo_frame32_sinks):
@@ -257,13 +264,14 @@ def _fill(box, cid, shift_col, sx, sy, sz, starts, shift):
     return src, dst
 
 
-def ref_gpu_slab(box, softening, eps, slab, repeats=1, b2=0.0, R=2):
-    """The reference GPU kernel on one whole x-slab as one SIC: returns
-    (acc float32[n_slab, 3] in particle order, mean launch ms, DirectTotal
-    pairs).  Sink pencil (y=j, z centre k): cells (slab, j, k-R..k+R) with z
-    shifted by (c-R) h; source pencil (j', k): cells (slab-R..slab+R, j', k)
-    with x shifted by (c-R) h; the y shift (y-R) h is applied on the device.
-    The five pencil partials of each sink are co-added in float32."""
+def sic_arrays(box, slab, R=2):
+    """The arrays of one whole x-slab as one SIC (PencilOnPencil.cc:254-416,
+    PencilPlan.cc:22-90, 214-255).  Sink pencil (y=j, z centre k): cells
+    (slab, j, k-R..k+R) with z shifted by (c-R) h, padded to 64-slot blocks;
+    source pencil (j', k): cells (slab-R..slab+R, j', k) with x shifted by
+    (c-R) h; sink pencil (j, k) meets source pencils (j+y-R, k), y = 0..2R,
+    with y offset (y-R) h.  s_src / s_dst map each sink's particle index to
+    its slot in each of its 2R+1 sink pencils."""
     f32 = np.float32
     cpd, W = box.cpd, 2 * R + 1
     h = f32(1.0 / cpd)
@@ -297,12 +305,51 @@ def ref_gpu_slab(box, softening, eps, slab, repeats=1, b2=0.0, R=2):
     ys = np.arange(W)
     ilist = (((j[:, None] + ys[None, :] - R) % cpd) * cpd + k[:, None]).astype(np.int32)
     yoff = np.tile(shift, (P, 1)).astype(np.float32)
-    # every index the kernel will use, checked on the host before the launch
+    # every index a kernel will use, checked on the host
     assert parent.size == nslots // 64
     assert np.all(id_max <= nslots) and np.all(s_start % 64 == 0)
     assert np.all((ilist >= 0) & (ilist < P))
     assert np.all(q_start + n_q <= nsrc)
     assert nslots < 2 ** 31 and nsrc < 2 ** 31
+    return SimpleNamespace(P=P, W=W, nblk=nblk, nslots=nslots, nsrc=nsrc, sx=sx, sy=sy, sz=sz,
+                           tx=tx, ty=ty, tz=tz, id_max=id_max, parent=parent, q_start=q_start,
+                           n_q=n_q, ilist=ilist, yoff=yoff, s_src=s_src, s_dst=s_dst, n_p=n_p)
+
+
+def _coadd(box, slab, a, acc):
+    """Each sink's 2R+1 pencil partials summed in float32, in pencil order."""
+    p0, p1 = box.slab_range(slab)
+    out = np.zeros((p1 - p0, 3), np.float32)
+    np.add.at(out, a.s_src - p0, acc[a.s_dst, :3])
+    return out
+
+
+def cpu_execute_slab(box, eps, slab, R=2):
+    """SetInteractionCollection::CPUExecute (Plummer) on one whole x-slab as
+    one SIC: float32[n_slab, 3] in particle order."""
+    a = sic_arrays(box, slab, R)
+    acc = np.zeros((max(a.nslots, 1), 3), np.float32)
+    sink_xyz = np.ascontiguousarray(np.concatenate([a.sx, a.sy, a.sz]))
+    src_xyz = np.ascontiguousarray(np.concatenate([a.tx, a.ty, a.tz]))
+    _check(lib().nfo_cpu_execute(int(a.nblk.sum()), a.nslots, sink_xyz, a.id_max, a.parent,
+                                 a.nsrc, src_xyz, a.q_start.astype(np.int32),
+                                 a.n_q.astype(np.int32),
+                                 np.ascontiguousarray(a.ilist.ravel()),
+                                 np.ascontiguousarray(a.yoff.ravel()), a.W, float(np.float32(eps)),
+                                 acc.reshape(-1)))
+    return _coadd(box, slab, a, acc)
+
+
+def ref_gpu_slab(box, softening, eps, slab, repeats=1, b2=0.0, R=2):
+    """The reference GPU kernel on one whole x-slab as one SIC (the arrays of
+    sic_arrays): returns (acc float32[n_slab, 3] in particle order, mean
+    launch ms, DirectTotal pairs).  The y shift is applied on the device; the
+    five pencil partials of each sink are co-added in float32."""
+    a = sic_arrays(box, slab, R)
+    P, nblk, nslots, nsrc = a.P, a.nblk, a.nslots, a.nsrc
+    sx, sy, sz, tx, ty, tz = a.sx, a.sy, a.sz, a.tx, a.ty, a.tz
+    id_max, parent, q_start, n_q, ilist, yoff = a.id_max, a.parent, a.q_start, a.n_q, a.ilist, a.yoff
+    f32 = np.float32
     L = ref_gpu_lib(softening)
     nf4 = L.nfrefgpu_accstruct_floats()
     acc = np.zeros((max(nslots, 1), nf4), f32)
@@ -311,7 +358,7 @@ def ref_gpu_slab(box, softening, eps, slab, repeats=1, b2=0.0, R=2):
     q_start32 = q_start.astype(np.int32)
     n_q32 = n_q.astype(np.int32)
     ms = ctypes.c_float(0)
-    ptr = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+    ptr = lambda v: v.ctypes.data_as(ctypes.c_void_p)
     rc = L.nfrefgpu_run(int(nblk.sum()), nslots, ptr(sink_xyz), ptr(id_max), ptr(parent), nsrc,
                         ptr(src_xyz), P, ptr(q_start32), ptr(n_q32), int(ilist.size),
                         ptr(np.ascontiguousarray(ilist.ravel())),
@@ -319,8 +366,5 @@ def ref_gpu_slab(box, softening, eps, slab, repeats=1, b2=0.0, R=2):
                         float(np.float32(b2)), int(repeats), ptr(acc), ctypes.byref(ms))
     if rc != 0:
         raise RuntimeError(f"reference GPU kernel failed: cudaError {rc}")
-    p0, p1 = box.slab_range(slab)
-    out = np.zeros((p1 - p0, 3), f32)
-    np.add.at(out, s_src - p0, acc[s_dst, :3])
-    pairs = int((n_p[:, None] * n_q[ilist]).sum())
-    return out, ms.value, pairs
+    pairs = int((a.n_p[:, None] * n_q[ilist]).sum())
+    return _coadd(box, slab, a, acc), ms.value, pairs
