@@ -460,28 +460,27 @@ class AbacusNodeSlabs:
     def __init__(self, box, zs: int, zn: int, R: int = 2, record_width: int = 4):
         cpd = self.cpd = box.cpd
         c2 = cpd * cpd
-        zcells = [(zs + dz) % cpd for dz in range(-R, zn + R)]
+        zcells = (zs + np.arange(-R, zn + R)) % cpd          # row order: ghosts, primary, ghosts
+        primary = np.zeros(len(zcells), bool)
+        primary[R:R + zn] = True
         self.posxyz, self.cellinfo, self.acc, self.maps, self.nslab = [], [], [], [], []
         self.mask = np.zeros(box.n, bool)
+        cs = np.asarray(box.cell_start, np.int64)
         for s in range(cpd):
+            cid = (s * c2 + np.arange(cpd)[:, None] * cpd + zcells[None, :]).ravel()
+            a, n = cs[cid], cs[cid + 1] - cs[cid]             # (y, z-in-row) order
+            prim = np.tile(primary, cpd)
+            start_g = np.concatenate([[0], np.cumsum(n)[:-1]])
+            npri = np.where(prim, n, 0)
+            start_p = np.concatenate([[0], np.cumsum(npri)[:-1]])
             ci = np.zeros(c2, dtype=CELLINFO_DTYPE)
-            pos, acc_map = [], []
-            ng = npri = 0
-            for y in range(cpd):
-                for i, z in enumerate(zcells):
-                    c = (s * cpd + y) * cpd + z
-                    a, b = int(box.cell_start[c]), int(box.cell_start[c + 1])
-                    ci[y * cpd + z]["startindex_with_ghost"] = ng
-                    ci[y * cpd + z]["startindex"] = npri
-                    ci[y * cpd + z]["count"] = b - a
-                    ci[y * cpd + z]["active"] = b - a
-                    pos.append(np.arange(a, b))
-                    ng += b - a
-                    if R <= i < R + zn:
-                        acc_map.append(np.arange(a, b))
-                        npri += b - a
-            idx = np.concatenate(pos) if pos else np.zeros(0, np.int64)
-            amap = np.concatenate(acc_map) if acc_map else np.zeros(0, np.int64)
+            local = cid - s * c2
+            ci["startindex_with_ghost"][local] = start_g
+            ci["startindex"][local] = start_p
+            ci["count"][local] = n
+            ci["active"][local] = n
+            idx = np.repeat(a, n) + (np.arange(int(n.sum())) - np.repeat(start_g, n))
+            amap = idx[np.repeat(prim, n)]
             self.mask[amap] = True
             self.posxyz.append(np.ascontiguousarray(
                 np.concatenate([box.x[idx], box.y[idx], box.z[idx]]), dtype=np.float32))
