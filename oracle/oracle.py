@@ -240,11 +240,14 @@ def ref_gpu_lib(softening: int):
     return _ref_gpu_libs[softening]
 
 
-def _fill(box, cid, shift_col, sx, sy, sz, starts, shift):
+def _fill(box, cid, shift_col, sx, sy, sz, starts, shift, keep=None):
     """Copy the particles of cells cid[p, c] into slots starts[p] + running
-    offset, adding shift[c] to the coordinate shift_col (0: x, 2: z)."""
+    offset, adding shift[c] to the coordinate shift_col (0: x, 2: z); cells
+    with keep[p, c] False contribute nothing."""
     cs = box.cell_start
     n = (cs[cid + 1] - cs[cid]).astype(np.int64)
+    if keep is not None:
+        n = np.where(keep, n, 0)
     P, W = cid.shape
     off = np.zeros_like(n)
     off[:, 1:] = np.cumsum(n, axis=1)[:, :-1]
@@ -264,33 +267,43 @@ def _fill(box, cid, shift_col, sx, sy, sz, starts, shift):
     return src, dst
 
 
-def sic_arrays(box, slab, R=2):
+def sic_arrays(box, slab, R=2, node=None):
     """The arrays of one whole x-slab as one SIC (PencilOnPencil.cc:254-416,
     PencilPlan.cc:22-90, 214-255).  Sink pencil (y=j, z centre k): cells
     (slab, j, k-R..k+R) with z shifted by (c-R) h, padded to 64-slot blocks;
     source pencil (j', k): cells (slab-R..slab+R, j', k) with x shifted by
     (c-R) h; sink pencil (j, k) meets source pencils (j+y-R, k), y = 0..2R,
     with y offset (y-R) h.  s_src / s_dst map each sink's particle index to
-    its slot in each of its 2R+1 sink pencils."""
+    its slot in each of its 2R+1 sink pencils.
+    node = (node_z_start, node_z_size): one node of a 2D z-split -- centres
+    node_z_start-R .. node_z_start+node_z_size+R-1 (index_to_zcen with its
+    pad, PencilOnPencil.cc:37-43) and sink pencils truncated to the node's
+    primary cells (PencilPlan.cc:110-116)."""
     f32 = np.float32
     cpd, W = box.cpd, 2 * R + 1
     h = f32(1.0 / cpd)
     shift = np.array([f32(c - R) * h for c in range(W)], dtype=np.float32)
     cs = box.cell_start
     counts = np.diff(cs)
-    j = np.repeat(np.arange(cpd), cpd)
-    k = np.tile(np.arange(cpd), cpd)
-    P = cpd * cpd
+    centres = np.arange(cpd) if node is None else (node[0] + np.arange(-R, node[1] + R)) % cpd
+    nk = len(centres)
+    j = np.repeat(np.arange(cpd), nk)
+    kidx = np.tile(np.arange(nk), cpd)
+    k = centres[kidx]
+    P = cpd * nk
     cells = np.arange(W)
-    sink_cid = (slab * cpd + j[:, None]) * cpd + (k[:, None] + cells[None, :] - R) % cpd
-    n_p = counts[sink_cid].sum(axis=1)
+    sink_z = (k[:, None] + cells[None, :] - R) % cpd
+    sink_cid = (slab * cpd + j[:, None]) * cpd + sink_z
+    keep = None if node is None else (sink_z - node[0]) % cpd < node[1]
+    n_p = np.where(keep, counts[sink_cid], 0).sum(axis=1) if keep is not None \
+        else counts[sink_cid].sum(axis=1)
     padded = (n_p + 63) // 64 * 64
     s_start = np.concatenate([[0], np.cumsum(padded)[:-1]]).astype(np.int64)
     nslots = int(padded.sum())
     sx = np.zeros(nslots, f32)
     sy = np.zeros(nslots, f32)
     sz = np.zeros(nslots, f32)
-    s_src, s_dst = _fill(box, sink_cid, 2, sx, sy, sz, s_start, shift)
+    s_src, s_dst = _fill(box, sink_cid, 2, sx, sy, sz, s_start, shift, keep)
     id_max = (s_start + n_p).astype(np.uint32)
     nblk = padded // 64
     parent = np.repeat(np.arange(P), nblk).astype(np.int32)
@@ -303,7 +316,7 @@ def sic_arrays(box, slab, R=2):
     tz = np.zeros(nsrc, f32)
     _fill(box, src_cid, 0, tx, ty, tz, q_start, shift)
     ys = np.arange(W)
-    ilist = (((j[:, None] + ys[None, :] - R) % cpd) * cpd + k[:, None]).astype(np.int32)
+    ilist = (((j[:, None] + ys[None, :] - R) % cpd) * nk + kidx[:, None]).astype(np.int32)
     yoff = np.tile(shift, (P, 1)).astype(np.float32)
     # every index a kernel will use, checked on the host
     assert parent.size == nslots // 64
@@ -324,10 +337,11 @@ def _coadd(box, slab, a, acc):
     return out
 
 
-def cpu_execute_slab(box, eps, slab, R=2):
+def cpu_execute_slab(box, eps, slab, R=2, node=None):
     """SetInteractionCollection::CPUExecute (Plummer) on one whole x-slab as
-    one SIC: float32[n_slab, 3] in particle order."""
-    a = sic_arrays(box, slab, R)
+    one SIC: float32[n_slab, 3] in particle order (a 2D node: its primary
+    particles only, the rest zero)."""
+    a = sic_arrays(box, slab, R, node)
     acc = np.zeros((max(a.nslots, 1), 3), np.float32)
     sink_xyz = np.ascontiguousarray(np.concatenate([a.sx, a.sy, a.sz]))
     src_xyz = np.ascontiguousarray(np.concatenate([a.tx, a.ty, a.tz]))

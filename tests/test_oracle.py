@@ -137,3 +137,30 @@ def test_cpu_execute_pins_pencil_layout(oracle, synth, kind):
     rms, mx, _ = oracle.frac_errors(pen.astype(np.float64),
                                     oracle.fp64_sinks(box, 0, eps, np.arange(box.n)))
     assert rms <= 5e-6 and mx <= 1e-4, (rms, mx)
+
+
+def test_cpu_execute_2d_nodes_cover_the_box(oracle, synth):
+    """The 2D z-split on the reference's own pencil arithmetic: SICs of the
+    nodes of a z-partition (pencils centred over each node's cells and R
+    ghost cells each side, sink pencils truncated to its primary cells)
+    give every particle exactly once, and the same accelerations as one
+    z-domain up to the float32 order of the pencil co-add."""
+    box = synth.clustered_box(30000, 13, seed=83, n_clumps=20)
+    eps = synth.kernel_eps(0, synth.plummer_eps(31))
+    cpd = box.cpd
+    cellz = np.repeat(np.arange(cpd ** 3) % cpd, np.diff(box.cell_start))
+    one = np.zeros((box.n, 3), np.float32)
+    two = np.zeros((box.n, 3), np.float32)
+    cover = np.zeros(box.n, int)
+    for s in range(cpd):
+        p0, p1 = box.slab_range(s)
+        one[p0:p1] = oracle.cpu_execute_slab(box, eps, s)
+        for zs, zn in [(11, 5), (3, 4), (7, 4)]:
+            r = oracle.cpu_execute_slab(box, eps, s, node=(zs, zn))
+            prim = (cellz[p0:p1] - zs) % cpd < zn
+            assert np.all(r[~prim] == 0)
+            two[p0:p1][prim] = r[prim]
+            cover[p0:p1][prim] += 1
+    assert np.all(cover == 1)
+    norm = np.linalg.norm(one.astype(np.float64), axis=1)
+    assert np.all(np.abs(two.astype(np.float64) - one) <= 1e-5 * norm[:, None])
