@@ -354,12 +354,13 @@ def cpu_execute_slab(box, eps, slab, R=2, node=None):
     return _coadd(box, slab, a, acc)
 
 
-def ref_gpu_slab(box, softening, eps, slab, repeats=1, b2=0.0, R=2):
+def ref_gpu_slab(box, softening, eps, slab, repeats=1, b2=0.0, R=2, node=None):
     """The reference GPU kernel on one whole x-slab as one SIC (the arrays of
-    sic_arrays): returns (acc float32[n_slab, 3] in particle order, mean
-    launch ms, DirectTotal pairs).  The y shift is applied on the device; the
-    five pencil partials of each sink are co-added in float32."""
-    a = sic_arrays(box, slab, R)
+    sic_arrays; node: one node of a 2D z-split): returns (acc float32[n_slab,
+    3] in particle order, mean launch ms, DirectTotal pairs).  The y shift is
+    applied on the device; the five pencil partials of each sink are co-added
+    in float32."""
+    a = sic_arrays(box, slab, R, node)
     P, nblk, nslots, nsrc = a.P, a.nblk, a.nslots, a.nsrc
     sx, sy, sz, tx, ty, tz = a.sx, a.sy, a.sz, a.tx, a.ty, a.tz
     id_max, parent, q_start, n_q, ilist, yoff = a.id_max, a.parent, a.q_start, a.n_q, a.ilist, a.yoff

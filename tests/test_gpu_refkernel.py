@@ -39,6 +39,37 @@ def test_slabs_match_reference_gpu_kernel(capi, synth, oracle, softening):
         db.close()
 
 
+@pytest.mark.parametrize("softening", [0, 1])
+def test_2d_nodes_match_reference_gpu_kernel(capi, synth, oracle, softening):
+    """2D z-split: the drop-in driver on each node of a z-partition against
+    the reference kernel on the same nodes' SICs (sink pencils truncated to
+    the node's cells, ghost cells as sources)."""
+    if not oracle.have_ref_gpu(softening):
+        pytest.skip("reference GPU kernel not built (needs the reference sources)")
+    box = synth.clustered_box(50000, 13, seed=72, n_clumps=20)
+    length = synth.plummer_eps(37)
+    eps = synth.kernel_eps(softening, length)
+    cpd = box.cpd
+    cellz = np.repeat(np.arange(cpd ** 3) % cpd, np.diff(box.cell_start))
+    for zs, zn in [(11, 5), (3, 4), (7, 4)]:
+        drv = capi.Driver(box, softening=softening, softening_length=length, direct_bpd=2,
+                          node_z=(zs, zn))
+        try:
+            got = drv.run_all()[:, :3]
+        finally:
+            drv.close()
+        for slab in (0, 6, 12):
+            p0, p1 = box.slab_range(slab)
+            ref, _, _ = oracle.ref_gpu_slab(box, softening, eps, slab, node=(zs, zn))
+            prim = (cellz[p0:p1] - zs) % cpd < zn
+            r, g = ref[prim].astype(np.float64), got[p0:p1][prim].astype(np.float64)
+            norm = np.linalg.norm(r, axis=1)
+            ok = norm > 0
+            diff = np.abs(g - r)
+            assert np.all(diff[ok] <= 1e-4 * norm[ok, None]), \
+                float((diff[ok] / norm[ok, None]).max())
+
+
 def test_reference_kernel_bar(capi, synth, oracle):
     if not oracle.have_ref_gpu(1):
         pytest.skip("reference GPU kernel not built (needs the reference sources)")
