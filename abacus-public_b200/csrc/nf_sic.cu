@@ -303,7 +303,17 @@ static nf_status run_task(nf_ctx *ctx, SicBuffer &b, const SicTask &t) {
     for (int s = 0; s < W; s++) {
         const float *slab = d.source_pos_slab[s];
         const uint64_t ns = d.source_nslab[s];
-        for (int y = 0; y < cpd && two_d; y++) {  // 2D: cell by cell (ghost cells included)
+        // 2D: cell by cell (ghost cells included), cells that follow each
+        // other in both the slab and the mini box copied as one run
+        int64_t run_src = 0, run_dst = 0, run_n = 0;
+        auto flush = [&]() {
+            if (run_n == 0) return;
+            memcpy(hx + run_dst, slab + run_src, run_n * sizeof(float));
+            memcpy(hy + run_dst, slab + ns + run_src, run_n * sizeof(float));
+            memcpy(hz + run_dst, slab + 2 * ns + run_src, run_n * sizeof(float));
+            run_n = 0;
+        };
+        for (int y = 0; y < cpd && two_d; y++) {
             if (!row_used[y]) continue;
             for (int z = 0; z < cpd; z++) {
                 const int64_t c = ((int64_t)s * cpd + y) * cpd + z;
@@ -313,11 +323,17 @@ static nf_status run_task(nf_ctx *ctx, SicBuffer &b, const SicTask &t) {
                     set_error("nf_sic_execute: source cell outside its slab");
                     return NF_EINVAL;
                 }
-                memcpy(hx + dst, slab + src, n * sizeof(float));
-                memcpy(hy + dst, slab + ns + src, n * sizeof(float));
-                memcpy(hz + dst, slab + 2 * ns + src, n * sizeof(float));
+                if (run_n > 0 && src == run_src + run_n && dst == run_dst + run_n) {
+                    run_n += n;
+                } else {
+                    flush();
+                    run_src = src;
+                    run_dst = dst;
+                    run_n = n;
+                }
             }
         }
+        flush();
         for (int y = 0; y < cpd && !two_d; y++) {
             if (!row_used[y]) continue;
             int64_t dst = cs[((int64_t)s * cpd + y) * cpd];
@@ -366,7 +382,13 @@ static nf_status run_task(nf_ctx *ctx, SicBuffer &b, const SicTask &t) {
     NF_CUDA(cudaStreamSynchronize(sm));
     if (two_d) {
         // primary cells only, each at its AccSlab start (the centre cell of
-        // the pencil centred on it)
+        // the pencil centred on it); cells adjacent in both go as one run
+        size_t run_acc = 0, run_out = 0, run_bytes = 0;
+        auto flush = [&]() {
+            if (run_bytes)
+                memcpy((char *)d.sink_acc_slab + run_acc, (char *)b.h_out + run_out, run_bytes);
+            run_bytes = 0;
+        };
         for (int j = 0; j < jw; j++)
             for (int k = 0; k < nk; k++) {
                 const int y = t.jlow + j, zc = zcen(k);
@@ -377,10 +399,19 @@ static nf_status run_task(nf_ctx *ctx, SicBuffer &b, const SicTask &t) {
                     set_error("nf_sic_execute: sink plan and source plan disagree on a cell");
                     return NF_EINVAL;
                 }
-                if (ce.n)
-                    memcpy((char *)d.sink_acc_slab + (size_t)ce.start * rec,
-                           (char *)b.h_out + (size_t)(cs[c] - p0) * rec, (size_t)ce.n * rec);
+                if (ce.n == 0) continue;
+                const size_t acc = (size_t)ce.start * rec, out = (size_t)(cs[c] - p0) * rec;
+                const size_t bytes = (size_t)ce.n * rec;
+                if (run_bytes && acc == run_acc + run_bytes && out == run_out + run_bytes) {
+                    run_bytes += bytes;
+                } else {
+                    flush();
+                    run_acc = acc;
+                    run_out = out;
+                    run_bytes = bytes;
+                }
             }
+        flush();
     } else if (n_sinks > 0) {
         // AccSlab rows [jlow, jhigh) are contiguous from the first sink cell of row jlow
         // the centre cell of the row-jlow pencil centred on z = 0 is cell (jlow, 0)
