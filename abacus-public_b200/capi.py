@@ -24,6 +24,7 @@ STATUS_NAMES = {0: "NF_OK", 1: "NF_EINVAL", 2: "NF_ENOMEM", 3: "NF_EADMISSION",
 SOFT_PLUMMER, SOFT_SINGLE_SPLINE, SOFT_CUBIC_SPLINE, SOFT_CUBIC_PLUMMER = range(4)
 ACC_COMPENSATED, ACC_PLAIN = 0, 1
 OUT_FLOAT3, OUT_FLOAT4 = 0, 1
+ABI_VERSION = 2  # NF_ABI_VERSION of include/nf_capi.h
 
 
 class NfError(RuntimeError):
@@ -247,6 +248,9 @@ def lib():
             fn = getattr(L, name)  # AttributeError if not exported
             fn.restype = res
             fn.argtypes = args
+        if L.nf_abi_version() != ABI_VERSION:
+            raise RuntimeError(f"{LIB_PATH} has ABI version {L.nf_abi_version()}, this binding "
+                               f"expects {ABI_VERSION}: rebuild it with abacus-public_b200/build.py")
         _lib = L
     return _lib
 

@@ -45,7 +45,8 @@
 extern "C" {
 #endif
 
-#define NF_ABI_VERSION 1
+/* 2: nf_sic_desc and nf_driver_params end with node_z_start, node_z_size. */
+#define NF_ABI_VERSION 2
 
 /* ---------------- status codes ---------------- */
 typedef int nf_status;

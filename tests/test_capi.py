@@ -13,7 +13,7 @@ def test_library_exports_every_declared_symbol(capi):
 
 
 def test_abi_version_and_defaults(capi):
-    assert capi.lib().nf_abi_version() == 1
+    assert capi.lib().nf_abi_version() == capi.ABI_VERSION == 2
     c = capi.default_config()
     assert c.near_field_radius == 2
     assert c.softening == capi.SOFT_SINGLE_SPLINE
