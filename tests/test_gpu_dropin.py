@@ -136,3 +136,28 @@ def test_driver_2d_z_split(capi, oracle, synth, soft, nodes, out_kind):
     diff = np.abs(a2[:, :3].astype(np.float64) - a1[:, :3])
     assert np.all(diff[ok] <= 2e-6 * norm[ok, None]), float((diff[ok] / norm[ok, None]).max())
     _check(oracle, box, soft, eps, a2)
+
+
+@pytest.mark.parametrize("node", [None, (4, 6)])
+def test_every_record_written(capi, synth, node):
+    """ForceOutputDebug's check (singlestep/Timestep/directdriver.cpp:344-356):
+    AccSlab pre-filled with +inf, every sink record (of the node's primary
+    cells for a 2D node) must come back finite; the batched form's output,
+    pre-filled with NaN, likewise."""
+    box = synth.clustered_box(40000, 13, seed=45, n_clumps=25)
+    length = synth.plummer_eps(34)
+    drv = capi.Driver(box, softening=1, softening_length=length, direct_bpd=2, node_z=node)
+    try:
+        for a in drv.slabs.acc:
+            a[:] = np.inf
+        acc = drv.run_all()
+        mask = drv.slabs.mask if node else np.ones(box.n, bool)
+    finally:
+        drv.close()
+    assert np.all(np.isfinite(acc[mask]))
+    with capi.Context(softening=1, eps=synth.kernel_eps(1, length)) as ctx:
+        db = ctx.box(box)
+        out = np.full((box.n, db.record_width()), np.nan, np.float32)
+        db.forces(0, box.cpd, out=out)
+        db.close()
+    assert np.all(np.isfinite(out))
