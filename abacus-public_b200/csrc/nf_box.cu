@@ -1089,8 +1089,10 @@ extern "C" nf_status nf_box_create(nf_ctx *ctx, int cpd, int64_t np, const int64
         set_error("nf_box_create: cpd must be odd and >= 2R+1");
         return NF_EINVAL;
     }
-    if (np >= ((int64_t)1 << 31) || (int64_t)cpd * cpd * cpd >= ((int64_t)1 << 34)) {
-        set_error("nf_box_create: at most 2^31 - 1 particles and 2^34 cells per box");
+    // work items name a pencil by its centre cell's linear id in 32 bits
+    if (np >= ((int64_t)1 << 31) || (int64_t)cpd * cpd * cpd >= ((int64_t)1 << 31)) {
+        set_error("nf_box_create: at most 2^31 - 1 particles and cpd^3 < 2^31 cells "
+                  "(cpd <= 1290) per box");
         return NF_EINVAL;
     }
     int64_t ncell = (int64_t)cpd * cpd * cpd;
@@ -1715,6 +1717,11 @@ extern "C" nf_status nf_forces_noalloc(const nf_config *cfg, int cpd, const void
         (cfg->out_kind != NF_OUT_FLOAT3 && cfg->out_kind != NF_OUT_FLOAT4) ||
         (cfg->out_kind == NF_OUT_FLOAT3 && cfg->b2 > 0.f)) {
         set_error("nf_forces_noalloc: bad configuration or slab range");
+        return NF_EINVAL;
+    }
+    if ((int64_t)cpd * cpd * cpd >= ((int64_t)1 << 31)) {
+        // pencil ids (linear cell ids) are 32-bit in the work loop
+        set_error("nf_forces_noalloc: cpd^3 must be below 2^31 (cpd <= 1290)");
         return NF_EINVAL;
     }
     cudaStream_t st = (cudaStream_t)stream;

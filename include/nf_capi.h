@@ -471,12 +471,16 @@ nf_status nf_box_kick(nf_ctx *ctx, nf_box *box, int slab_lo, int slab_hi,
  *   out        device records (cfg->out_kind) for the particles of slabs
  *              [slab_lo, slab_hi), in particle order
  *   stream     a cudaStream_t, or NULL for the default stream
- * At most 196608 particles in the requested slabs; more is NF_EINVAL.  The
- * first call on each device looks up the array's device address with that
- * device current; make that first call before any stream capture.  All
- * calls share the one array and it keeps the last call's contents: calls
- * that overlap on the GPU (other streams, other host threads) race.  The
- * call returns once the work is queued on `stream`. */
+ * At most 196608 particles in the requested slabs, and cpd^3 < 2^31; more
+ * is NF_EINVAL.  The first call on each device looks up the array's device
+ * address with that device current; make that first call before any stream
+ * capture.  All calls share the one array and it keeps the last call's
+ * contents: calls that overlap on the GPU (other streams, other host
+ * threads) race.  Every call first copies the slab range's two particle
+ * bounds from cell_start to the host and synchronizes `stream` to read
+ * them, so the host waits for all earlier work on `stream`; the sweep and
+ * the co-add are then queued on `stream` and the call returns without
+ * waiting for them. */
 nf_status nf_forces_noalloc(const nf_config *cfg, int cpd, const void *pos,
                             const int64_t *cell_start, int slab_lo, int slab_hi, void *out,
                             void *stream);

@@ -26,3 +26,14 @@ def test_library_is_sm100a_only(capi):
     build recipe's flags, not by reading the binary)."""
     from abacus_public_b200 import build
     assert build.ARCH == ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def test_noalloc_rejects_boxes_beyond_32_bit_pencil_ids(capi):
+    """cpd^3 must stay below 2^31 (pencil ids are 32-bit): the call refuses
+    cpd = 1291 before it touches the device, so this runs without a GPU."""
+    cfg = capi.default_config(softening=0, eps=1e-6)
+    dummy = ctypes.c_void_p(16)
+    rc = capi.lib().nf_forces_noalloc(ctypes.byref(cfg), 1291, dummy, dummy, 0, 1, dummy,
+                                      ctypes.c_void_p(0))
+    assert rc == capi.NF_EINVAL
+    assert b"1290" in capi.lib().nf_last_error()

@@ -226,3 +226,16 @@ def test_errors_are_status_codes(capi, synth):
         with pytest.raises(capi.NfError):
             db.forces(0, 6)
         db.close()
+
+
+def test_box_rejects_cpd_beyond_32_bit_pencil_ids(capi):
+    """Work items name a pencil by its centre cell's 32-bit linear id, so a box
+    must have cpd^3 < 2^31: cpd = 1291 is refused before any cell is read."""
+    import ctypes
+    dummy = np.zeros(4, np.int64)
+    with capi.Context(softening=0, eps=1e-6) as ctx:
+        h = ctypes.c_void_p()
+        rc = capi.lib().nf_box_create(ctx.h, 1291, 0, dummy.ctypes.data_as(ctypes.c_void_p),
+                                      None, None, None, ctypes.byref(h))
+        assert rc == capi.NF_EINVAL and not h.value
+        assert "1290" in capi.last_error()
