@@ -198,6 +198,9 @@ EXPORTS = {
     "nf_sic_execute": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(SicDesc), ctypes.c_int,
                                       ctypes.c_int, ctypes.c_int, ctypes.c_void_p]),
     "nf_sic_drain": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64]),
+    "nf_sic_timing": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
+                                     ctypes.POINTER(ctypes.c_uint64),
+                                     ctypes.POINTER(ctypes.c_uint64), ctypes.c_int]),
     "nf_box_create": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int64,
                                      ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                      ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]),
@@ -549,6 +552,14 @@ class Driver:
         s = DriverStats()
         check(lib().nf_driver_aggregate_stats(self.h, ctypes.byref(s)), "AggregateStats")
         return s
+
+    def sic_timing(self, reset: bool = False) -> tuple[float, int, int]:
+        """(summed pencil-kernel ms, SICs, unpadded pairs) of the SICs run since
+        the last reset."""
+        ms, n, p = ctypes.c_double(), ctypes.c_uint64(), ctypes.c_uint64()
+        check(lib().nf_sic_timing(lib().nf_driver_context(self.h), ctypes.byref(ms),
+                                  ctypes.byref(n), ctypes.byref(p), int(reset)), "nf_sic_timing")
+        return ms.value, int(n.value), int(p.value)
 
     def plan_sic(self, slab: int, jlow: int, jhigh: int):
         s = SicSummary()

@@ -173,24 +173,26 @@ extern "C" nf_status nf_set_stream(nf_ctx *ctx, void *stream) {
     return NF_OK;
 }
 
-// FFMA throughput probe: 8 independent dependency chains per thread.
+// FP32 throughput probe: 8 independent chains of paired FMAs (f32x2, two
+// FMAs per instruction) per thread, 16 per loop trip, so that loop control
+// takes under 1 % of the issue slots and the FMA pipe alone sets the rate.
+constexpr int PEAK_CHAINS = 8, PEAK_UNROLL = 16;
+
 __global__ void ffma_peak_kernel(float *out, int iters, float a, float b) {
-    float x0 = threadIdx.x * 1e-3f, x1 = x0 + 0.1f, x2 = x0 + 0.2f, x3 = x0 + 0.3f;
-    float x4 = x0 + 0.4f, x5 = x0 + 0.5f, x6 = x0 + 0.6f, x7 = x0 + 0.7f;
+    float2 x[PEAK_CHAINS];
+#pragma unroll
+    for (int c = 0; c < PEAK_CHAINS; c++)
+        x[c] = make_float2(threadIdx.x * 1e-3f + 0.1f * c, threadIdx.x * 1e-3f - 0.1f * c);
+    const float2 a2 = make_float2(a, a), b2 = make_float2(b, b);
     for (int i = 0; i < iters; i++) {
 #pragma unroll
-        for (int u = 0; u < 8; u++) {
-            x0 = fmaf(x0, a, b);
-            x1 = fmaf(x1, a, b);
-            x2 = fmaf(x2, a, b);
-            x3 = fmaf(x3, a, b);
-            x4 = fmaf(x4, a, b);
-            x5 = fmaf(x5, a, b);
-            x6 = fmaf(x6, a, b);
-            x7 = fmaf(x7, a, b);
-        }
+        for (int u = 0; u < PEAK_UNROLL; u++)
+#pragma unroll
+            for (int c = 0; c < PEAK_CHAINS; c++) x[c] = __ffma2_rn(x[c], a2, b2);
     }
-    float s = ((x0 + x1) + (x2 + x3)) + ((x4 + x5) + (x6 + x7));
+    float s = 0.f;
+#pragma unroll
+    for (int c = 0; c < PEAK_CHAINS; c++) s += x[c].x + x[c].y;
     if (s == 1234.5f) out[blockIdx.x * blockDim.x + threadIdx.x] = s;  // keeps the chains live
 }
 
@@ -202,10 +204,11 @@ extern "C" nf_status nf_measure_fp32_peak(nf_ctx *ctx, double seconds_sustained,
     }
     std::lock_guard<std::mutex> lk(ctx->mu);
     NF_CUDA(cudaSetDevice(ctx->device));
-    const int threads = 256, blocks = ctx->sms * 8, iters = 16384;
+    const int threads = 256, blocks = ctx->sms * 8, iters = 4096;
     float *out = nullptr;
     NF_CUDA(cudaMalloc(&out, (size_t)blocks * threads * sizeof(float)));
-    const double flops = 2.0 * 64.0 * iters * (double)blocks * threads;
+    // FMA = 2 flops, two FMAs per paired instruction
+    const double flops = 2.0 * 2.0 * PEAK_CHAINS * PEAK_UNROLL * (double)iters * blocks * threads;
     cudaStream_t s = ctx->stream;
     float best = 1e30f;
     cudaError_t e = cudaSuccess;

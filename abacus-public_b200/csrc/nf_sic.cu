@@ -43,6 +43,7 @@ struct SicBuffer {
     int index = 0, device = 0;
     bool pinned = true;
     cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;  // around the pencil kernel of a SIC
     std::mutex mu;
     float *d_raw = nullptr;
     float4 *d_pos = nullptr;
@@ -86,6 +87,9 @@ static void release(SicBuffer &b) {
     host_free(b.h_cs, b.pinned);
     host_free(b.h_items, b.pinned);
     if (b.stream) cudaStreamDestroy(b.stream);
+    if (b.ev0) cudaEventDestroy(b.ev0);
+    if (b.ev1) cudaEventDestroy(b.ev1);
+    b.ev0 = b.ev1 = nullptr;
     b.d_raw = nullptr;
     b.d_pos = nullptr;
     b.d_cs = nullptr;
@@ -207,6 +211,14 @@ static nf_status check_desc(nf_ctx *ctx, const nf_sic_desc &d, int jlow, int jhi
     return NF_OK;
 }
 
+static uint64_t items_pairs(const std::vector<Item> &items) {
+    uint64_t p = 0;
+    for (const Item &it : items) p += (uint64_t)it.nsink * (uint64_t)(it.src_end - it.src_begin);
+    return p;
+}
+
+static void sic_account(nf_ctx *ctx, float kernel_ms, uint64_t pairs);
+
 static nf_status run_task(nf_ctx *ctx, SicBuffer &b, const SicTask &t) {
     const nf_sic_desc &d = t.d;
     nf_status st = check_desc(ctx, d, t.jlow, t.jhigh);
@@ -295,6 +307,11 @@ static nf_status run_task(nf_ctx *ctx, SicBuffer &b, const SicTask &t) {
                     Item{pencil, (int)(g_lo + b0), take, take <= 32 ? 1 : 2, 0, (int)M, 0, 0});
             }
         }
+    // longest tiles first (the order of execution does not change any
+    // result: every tile writes its own partials)
+    std::stable_sort(items.begin(), items.end(), [](const Item &a, const Item &b) {
+        return (int64_t)a.nsink * a.src_end > (int64_t)b.nsink * b.src_end;
+    });
     nitems = items.size();
     st = grow(ctx, b, (size_t)n_mini, (size_t)n_sinks, nitems, (size_t)ncell + 1);
     if (st != NF_OK) return st;
@@ -373,13 +390,18 @@ static nf_status run_task(nf_ctx *ctx, SicBuffer &b, const SicTask &t) {
     L.p0 = p0;
     L.n_range = n_sinks;
     L.variant = engine_plain_variant();
+    NF_CUDA(cudaEventRecord(b.ev0, sm));
     st = engine_launch(ctx, L, 1.0 / cpd, sm);
     if (st != NF_OK) return st;
+    NF_CUDA(cudaEventRecord(b.ev1, sm));
     st = engine_coadd(ctx, b.d_part, n_sinks, b.d_out, sm);
     if (st != NF_OK) return st;
     const size_t rec = ctx->cfg.out_kind == NF_OUT_FLOAT4 ? 16 : 12;
     NF_CUDA(cudaMemcpyAsync(b.h_out, b.d_out, (size_t)n_sinks * rec, cudaMemcpyDeviceToHost, sm));
     NF_CUDA(cudaStreamSynchronize(sm));
+    float kms = 0.f;
+    NF_CUDA(cudaEventElapsedTime(&kms, b.ev0, b.ev1));
+    sic_account(ctx, kms, items_pairs(items));
     if (two_d) {
         // primary cells only, each at its AccSlab start (the centre cell of
         // the pencil centred on it); cells adjacent in both go as one run
@@ -440,7 +462,17 @@ struct nf_ctx::Sic {
     nf_gpu_limits limits{};
     int cpd = 0;
     std::string error;  // first failure seen by a worker
+    // pencil-kernel time of completed SICs (CUDA events around each launch)
+    double kernel_ms = 0.0;
+    uint64_t sics = 0, pairs = 0;
 };
+
+void nf::sic_account(nf_ctx *ctx, float kernel_ms, uint64_t pairs) {
+    std::lock_guard<std::mutex> lk(ctx->sic->mu);
+    ctx->sic->kernel_ms += kernel_ms;
+    ctx->sic->sics++;
+    ctx->sic->pairs += pairs;
+}
 
 static void finish(nf_ctx *ctx, const SicTask &t, nf_status st) {
     if (st != NF_OK) {
@@ -554,6 +586,8 @@ extern "C" nf_status nf_gpu_setup(nf_ctx *ctx, int cpd, uint64_t max_buffer_byte
         b->pinned = pinned;
         cudaError_t e = cudaSetDevice(b->device);
         if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreate(&b->ev0);
+        if (e == cudaSuccess) e = cudaEventCreate(&b->ev1);
         if (e != cudaSuccess) {
             nf_status s2 = cuda_fail(e, "nf_gpu_setup");
             S->buffers.push_back(std::move(b));
@@ -632,5 +666,29 @@ extern "C" nf_status nf_sic_drain(nf_ctx *ctx, uint64_t timeout_ns) {
         S->error.clear();
         return NF_EDEVICE;
     }
+    return NF_OK;
+}
+
+extern "C" nf_status nf_sic_timing(nf_ctx *ctx, double *kernel_ms, uint64_t *sics,
+                                   uint64_t *pairs, int reset) {
+    if (!ctx) {
+        set_error("nf_sic_timing: null context");
+        return NF_EINVAL;
+    }
+    double ms = 0.0;
+    uint64_t n = 0, p = 0;
+    if (ctx->sic) {
+        std::lock_guard<std::mutex> lk(ctx->sic->mu);
+        ms = ctx->sic->kernel_ms;
+        n = ctx->sic->sics;
+        p = ctx->sic->pairs;
+        if (reset) {
+            ctx->sic->kernel_ms = 0.0;
+            ctx->sic->sics = ctx->sic->pairs = 0;
+        }
+    }
+    if (kernel_ms) *kernel_ms = ms;
+    if (sics) *sics = n;
+    if (pairs) *pairs = p;
     return NF_OK;
 }

@@ -1,19 +1,28 @@
 """Near-field direct-force benchmark (one JSON line on stdout, rank 0).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload clustered256|uniform64|clustered512]
+                    [--workload clustered512|clustered256|uniform64|...]
 
 A step is one full near-field sweep of a synthetic box (every sink of every
 x-slab against its 5x5x5 cell neighbourhood), the box's positions already
-resident in HBM.  The default workload is the clustered box: 256^3 particles,
-cpd 65, 40% uniform + 60% in 2000 seeded NFW clumps, single-spline softening
-at 1/40 of the mean spacing, float32, compensated accumulation.
+resident in HBM.  The default workload is the clustered box the target is set
+on: 512^3 particles, cpd 125, 40% uniform + 60% in 2000 seeded NFW clumps,
+single-spline softening at 1/40 of the mean spacing, float32, compensated
+accumulation.
 
 metric: pair interactions/s (unpadded pairs, PencilOnPencil.cc:412 counting),
-plus p50/p99 slab latency.  Multi-GPU (torchrun): every rank sweeps its own
-independent box of the same configuration (weak scaling, no data-path
-collective); the timed region is bracketed by a barrier and the time is the
-max over ranks.
+plus p50/p99 slab latency.  Beside the sweep the line carries, for the same
+box: the end-to-end rate through the C ABI from pinned host buffers, the
+plain drop-in (NearFieldDriver -> SICs, wall clock and summed kernel time),
+the reference's own GPU kernel on one SIC per slab, the compensated-vs-plain
+precision study against the FP64 oracle on 0.1% of the sinks, per-component
+parity against the reference CPU direct on a fixed seeded sample of rows,
+and the five-box serving workload.
+
+Multi-GPU (torchrun): one box split over the ranks by x-slab ranges with a
+2-slab halo exchanged over NCCL (strong scaling); --replicas runs one
+independent box per rank instead (weak scaling).  The timed region is
+bracketed by a barrier and the time is the max over ranks.
 """
 from __future__ import annotations
 
@@ -227,64 +236,74 @@ def aggregate(pairs_per_rank: float, ms_per_rank: float, world: int) -> tuple[fl
 # CPU baseline: the reference's own kernel compiled from its sources
 # (oracle/_ref, -Ofast), driven by the ExecuteSlabCPU cell loop
 # ---------------------------------------------------------------------------
-def cpu_reference_rate(box, w, target_s=10.0, seed=0):
-    """Pairs/s of the reference CPU direct on a seeded sample of sink cells,
-    all host threads.  Returns (rate, threads, sample description, kind)."""
+CPU_SAMPLE_SEED = 123
+
+
+def cell_pairs(box, R=2):
+    """Pairs of every sink cell (its count times the count of its (2R+1)^3
+    neighbourhood, periodic), shape (cpd, cpd, cpd); sums to DirectTotal."""
+    cpd = box.cpd
+    c3 = box.counts.reshape(cpd, cpd, cpd).astype(np.int64)
+    nb = c3
+    for axis in range(3):
+        nb = sum(np.roll(nb, d, axis=axis) for d in range(-R, R + 1))
+    return c3 * nb
+
+
+def cpu_sample(box, target_pairs, seed=CPU_SAMPLE_SEED):
+    """A fixed seeded sample for the CPU reference: whole (x, y) rows of cells
+    (the unit of ExecuteSlabCPU's loop over y, extras_directdriver.cpp:59-122)
+    in a seeded order until target_pairs is reached (the whole box if it holds
+    fewer).  Both bench arms take the same rows.  Returns (cells, sinks,
+    pairs, description)."""
+    cpd = box.cpd
+    rows = cell_pairs(box).sum(axis=2).ravel()  # row x*cpd + y
+    order = np.random.default_rng(seed).permutation(rows.size)
+    cum = np.cumsum(rows[order])
+    k = min(int(np.searchsorted(cum, target_pairs)) + 1, rows.size)
+    chosen = np.sort(order[:k])
+    cells = (chosen[:, None] * cpd + np.arange(cpd)[None, :]).ravel()
+    cs = box.cell_start
+    cells = cells[cs[cells + 1] > cs[cells]]
+    n = (cs[cells + 1] - cs[cells]).astype(np.int64)
+    sinks = np.repeat(cs[cells] - np.cumsum(n) + n, n) + np.arange(int(n.sum()))
+    pairs = int(rows[chosen].sum())
+    desc = (f"{k} seeded (x, y) rows of cells (seed {seed}; {cells.size} non-empty cells, "
+            f"{sinks.size} sinks, {pairs:.4e} pairs)")
+    return cells, sinks, pairs, desc
+
+
+def cpu_reference_run(box, w, cells, threads):
+    """The reference CPU direct on the sample's cells: (float32[N, 3] with the
+    sample's rows written, seconds, kind)."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle
-    soft = w["softening"]
-    eps = kernel_eps(w)
-    threads = oracle.host_threads()
+    soft, eps = w["softening"], kernel_eps(w)
+    acc = np.zeros((box.n, 3), np.float32)
+    t0 = time.perf_counter()
     if oracle.have_ref(soft, "fast"):
+        oracle.ref_cells(box, soft, eps, cells, flavour="fast", threads=threads, acc=acc)
         kind = "reference"
-
-        def run(cells):
-            oracle.ref_cells(box, soft, eps, cells, flavour="fast", threads=threads)
     else:
+        oracle.ref32_cells(box, soft, eps, cells, acc=acc)
         kind = "port"
+    return acc, time.perf_counter() - t0, kind
 
-        def run(cells):
-            oracle.ref32_cells(box, soft, eps, cells)
-    counts = box.counts
-    ncell = counts.size
-    cpd = box.cpd
-    rng = np.random.default_rng(seed)
-    order = rng.permutation(np.nonzero(counts)[0])
 
-    def pairs_of(cells):
-        tot = 0
-        c3 = counts.reshape(cpd, cpd, cpd)
-        for c in cells:
-            cz, cy, cx = c % cpd, (c // cpd) % cpd, c // (cpd * cpd)
-            xs = [(cx + d) % cpd for d in range(-2, 3)]
-            ys = [(cy + d) % cpd for d in range(-2, 3)]
-            zs = [(cz + d) % cpd for d in range(-2, 3)]
-            tot += int(counts[c]) * int(c3[np.ix_(xs, ys, zs)].sum())
-        return tot
-
-    # calibrate on a small sample, then size the sample to ~target_s
-    n = max(threads * 4, 64)
-    cells = order[:n]
-    t0 = time.perf_counter()
-    run(cells)
-    dt = time.perf_counter() - t0
-    p = pairs_of(cells)
-    rate0 = p / max(dt, 1e-9)
-    want = rate0 * target_s
-    k = n
-    acc = p
-    while acc < want and k < ncell:
-        step = order[k:k + 4096]
-        acc += pairs_of(step)
-        k += step.size
-    cells = order[:k]
-    t0 = time.perf_counter()
-    run(cells)
-    dt = time.perf_counter() - t0
-    pairs = pairs_of(cells)
-    desc = (f"{k} seeded random non-empty sink cells of the same box "
-            f"({pairs:.3e} pairs, {dt:.1f} s), {threads} threads")
-    return pairs / dt, threads, desc, kind, pairs, dt
+def parity_vs_reference(a_gpu, a_ref, sinks, tol=1e-4):
+    """Per sink and component |a - a_ref| <= tol |a_ref| (vector norm of the
+    reference's acceleration), on the sample's sinks."""
+    ref = a_ref[sinks].astype(np.float64)
+    got = np.asarray(a_gpu[sinks, :3], np.float64)
+    norm = np.linalg.norm(ref, axis=1)
+    dev = np.abs(got - ref).max(axis=1)
+    ok = norm > 0
+    rel = dev[ok] / norm[ok]
+    vrel = np.linalg.norm(got - ref, axis=1)[ok] / norm[ok]
+    return {"sinks": int(sinks.size), "tolerance": f"|a - a_ref|_c <= {tol:g} |a_ref|",
+            "max_comp_rel": float(rel.max()) if rel.size else 0.0,
+            "rms_rel": float(np.sqrt(np.mean(vrel ** 2))) if vrel.size else 0.0,
+            "pass": bool(np.all(dev <= tol * norm))}
 
 
 def reference_arm(args, w):
@@ -298,26 +317,14 @@ def reference_arm(args, w):
     box = make_box(w)
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle
-    soft = w["softening"]
-    eps = kernel_eps(w)
     threads = oracle.host_threads()
-    flavour_ok = oracle.have_ref(soft, "fast")
-    # per step: a fixed seeded sample of sink cells sized to ~6 s on this host
-    rate, threads, desc, kind, pairs, dt = cpu_reference_rate(box, w, target_s=6.0, seed=123)
-    counts = box.counts
-    rng = np.random.default_rng(123)
-    order = rng.permutation(np.nonzero(counts)[0])
-    ncells = int(desc.split()[0])
-    cells = order[:ncells]
-    times = []
+    # per step: the fixed seeded sample of rows the other arm reports
+    cells, sinks, pairs, desc = cpu_sample(box, args.cpu_pairs)
+    times, kind = [], "port"
     for i in range(args.warmup + args.steps):
-        t0 = time.perf_counter()
-        if flavour_ok:
-            oracle.ref_cells(box, soft, eps, cells, flavour="fast", threads=threads)
-        else:
-            oracle.ref32_cells(box, soft, eps, cells)
+        _, dt, kind = cpu_reference_run(box, w, cells, threads)
         if i >= args.warmup:
-            times.append(time.perf_counter() - t0)
+            times.append(dt)
     ms = 1e3 * sum(times) / len(times)
     value = pairs / (ms / 1e3)
     line = {
@@ -326,8 +333,8 @@ def reference_arm(args, w):
         "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic",
         "config": {"workload": args.workload, "desc": w["desc"],
-                   "step": "a seeded sample of sink cells of the box (the reference CPU "
-                           "direct is too slow for whole sweeps)"},
+                   "step": "the reference CPU direct on a fixed seeded sample of whole rows "
+                           "of cells of the box (a whole sweep takes hours on the host)"},
         "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": threads, "kind": kind,
                          "sample": desc},
         "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0,
@@ -341,10 +348,13 @@ def percentile(xs, q):
     return float(np.percentile(np.asarray(xs), q)) if xs else None
 
 
-def plain_dropin(capi, box, w, device, steps=2):
-    """Pairs/s of the plain drop-in: the NearFieldDriver mirror (SIC planning,
-    y-splits, one launch per SIC, host slabs staged per SIC, AccSlab written
-    back) over every slab of the box; wall clock per full sweep."""
+def plain_dropin(capi, box, w, device, a_batched=None, steps=2):
+    """The plain drop-in: the NearFieldDriver mirror (SIC planning, y-splits,
+    one launch per SIC, host slabs staged per SIC, AccSlab written back) over
+    every slab of the box.  Wall clock per full sweep with DirectBPD 3, then
+    one sweep with DirectBPD 1 (SICs one after another) for the summed
+    pencil-kernel time of its SICs.  a_batched: the batched sweep's result, to
+    compare the drop-in's output with."""
     from abacus_public_b200 import synth
     length = synth.plummer_eps(w["n_side"])
     drv = capi.Driver(box, softening=w["softening"], softening_length=length, device=device,
@@ -354,59 +364,111 @@ def plain_dropin(capi, box, w, device, steps=2):
         times = []
         for _ in range(steps):
             t0 = time.perf_counter()
-            drv.run_all()
+            acc = drv.run_all()
             times.append(time.perf_counter() - t0)
         st = drv.stats()
         pairs = st.direct_interactions // (steps + 1)
         sec = float(np.mean(times))
-        return {"value": pairs / sec, "unit": "pairs/s", "ms_per_step": 1e3 * sec,
-                "splits_per_slab": st.mean_splits_per_slab, "buffers": st.nbuffers,
-                "gb_to_device_per_step": st.total_gb_to / (steps + 1),
-                "what": "host slabs -> NearFieldDriver -> SIC -> AccSlab, wall clock"}
+        res = {"value": pairs / sec, "unit": "pairs/s", "ms_per_step": 1e3 * sec,
+               "splits_per_slab": st.mean_splits_per_slab, "buffers": st.nbuffers,
+               "gb_to_device_per_step": st.total_gb_to / (steps + 1),
+               "what": "host slabs -> NearFieldDriver -> SIC -> AccSlab, wall clock"}
+        if a_batched is not None:
+            ref = np.asarray(a_batched[:, :3], np.float64)
+            norm = np.maximum(np.linalg.norm(ref, axis=1), 1e-300)
+            res["max_comp_rel_vs_batched"] = float(
+                (np.abs(acc[:, :3] - ref).max(axis=1) / norm).max())
+        del acc
     finally:
         drv.close()
+    drv = capi.Driver(box, softening=w["softening"], softening_length=length, device=device,
+                      direct_bpd=1)
+    try:
+        drv.run_all()
+        drv.sic_timing(reset=True)
+        drv.run_all()
+        kms, nsic, kpairs = drv.sic_timing()
+    finally:
+        drv.close()
+    res["kernel"] = {"pairs_per_s": kpairs / (kms / 1e3), "kernel_ms": kms, "sics": nsic,
+                     "pairs": kpairs,
+                     "what": "summed pencil-kernel time of the drop-in's SICs (DirectBPD 1, "
+                             "CUDA events around each SIC's launch)"}
+    return res
 
 
-def serving_phase(capi, ctx, db_main, w, args, rank, loads=(0.5, 1.0, 1.5), seed=7):
-    """Seeded Poisson slab requests over several boxes resident on the same
-    GPU, at fractions of the measured closed-loop capacity; p50/p99 latency
-    from submission to the result in the caller's device buffer.  Boxes: the
-    main box and a clustered 64*45^3 box, or (`--serve-boxes 45,65,...`)
-    clustered boxes of N = 64*cpd^3 for each listed cpd, each with its own
-    softening at 1/40 of its mean spacing."""
+def ref_gpu_leg(box, w, a_batched):
+    """The reference's own GPU kernel (ComputeDirects, PencilKernel.cu:97-188,
+    compiled from its sources for sm_100a) on every x-slab of the box as one
+    SIC, each laid out on the host as PencilOnPencil.cc / PencilPlan.cc do
+    while the previous slab runs: pairs / summed launch time, and the largest
+    per-component deviation of its forces from the batched sweep's."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+    from concurrent.futures import ThreadPoolExecutor
+    soft, eps = w["softening"], kernel_eps(w)
+    if not oracle.have_ref_gpu(soft):
+        return {"unavailable": "the reference GPU kernel is not built for this softening"}
+    tot_ms, pairs, worst = 0.0, 0, 0.0
+    with ThreadPoolExecutor(1) as ex:
+        fut = ex.submit(oracle.sic_arrays, box, 0)
+        for s in range(box.cpd):
+            arr = fut.result()
+            if s + 1 < box.cpd:
+                fut = ex.submit(oracle.sic_arrays, box, s + 1)
+            acc, ms, p = oracle.ref_gpu_run(box, soft, eps, s, arr, repeats=1)
+            del arr
+            tot_ms += ms
+            pairs += p
+            p0, p1 = box.slab_range(s)
+            ref = acc.astype(np.float64)
+            norm = np.linalg.norm(ref, axis=1)
+            ok = norm > 0
+            if ok.any():
+                dev = np.abs(np.asarray(a_batched[p0:p1, :3], np.float64) - ref).max(axis=1)
+                worst = max(worst, float((dev[ok] / norm[ok]).max()))
+    return {"value": pairs / (tot_ms / 1e3), "unit": "pairs/s", "kernel_ms": tot_ms,
+            "pairs": pairs, "sics": box.cpd, "max_comp_rel_vs_batched": worst,
+            "what": "reference ComputeDirects (PencilKernel.cu) built for sm_100a with its "
+                    "default GPU flags, one SIC per x-slab, summed CUDA-event launch time"}
+
+
+def serving_phase(capi, ctx, w, args, rank, seed=7):
+    """Seeded Poisson slab requests over several clustered boxes resident on
+    the same GPU, at fractions of the measured closed-loop capacity; p50/p99
+    latency from submission to the result in the caller's device buffer,
+    split into queue and run time.  Boxes: N = 64*cpd^3 for each cpd of
+    --serve-boxes (default 45, 65, 85, 105, 125), generated on the device,
+    each with its own softening at 1/40 of its mean spacing."""
     import torch
     from abacus_public_b200 import synth
     soft = w["softening"]
-    own = []
-    if args.serve_boxes:
-        cpds = [int(c) for c in args.serve_boxes.split(",")]
-        dbs, names = [], []
-    else:
-        cpds = [45]
-        dbs, names = [db_main], [f"{w['n_side']}^3 cpd {db_main.cpd}"]
+    cpds = [int(c) for c in args.serve_boxes.split(",")]
+    dbs, names = [], []
     for k, c in enumerate(cpds):
-        other = synth.clustered_box(64 * c ** 3, c, seed=100 + 17 * k + rank)
-        d = ctx.box(other)
+        x, y, z, cs = synth.clustered_box_device(64 * c ** 3, c, seed=100 + 17 * k + rank)
+        d = ctx.box(synth.Box(c, x, y, z, cs, f"serve cpd {c}"))
+        del x, y, z
         d.set_eps(synth.kernel_eps(soft, synth.plummer_eps(4 * c)))  # 64 per cell: spacing h/4
-        own.append(d)
         dbs.append(d)
         names.append(f"64*{c}^3 cpd {c} clustered")
+    torch.cuda.empty_cache()
     slabs = [(i, s) for i, d in enumerate(dbs) for s in range(d.cpd)]
     outs = {}
     for i, s in slabs:
         p0, p1 = dbs[i].slab_particles(s, s + 1)
         outs[(i, s)] = torch.empty((max(p1 - p0, 1), 4), dtype=torch.float32, device="cuda")
     rng = np.random.default_rng(seed)
-    per_level = args.serve_requests
+    n_req = args.serve_requests
     levels = []
-    with capi.Server(ctx, max_inflight=8) as srv:
+    with capi.Server(ctx, max_inflight=args.serve_slots) as srv:
         for _ in range(2):  # warm-up (plans, tuning); the second pass gives capacity
             t0 = time.perf_counter()
             tk = [srv.submit(dbs[i], s, outs[(i, s)].data_ptr(), True) for i, s in slabs]
             for t in tk:
-                srv.wait(t)
+                srv.wait(t, timeout_s=600.0)
             cap = len(slabs) / (time.perf_counter() - t0)
-        for load in loads:
+        for load, per_level in ((0.5, n_req), (1.0, n_req), (1.5, max(n_req // 2, 1))):
             rate = load * cap
             arr = np.cumsum(rng.exponential(1.0 / rate, per_level))
             pick = rng.integers(0, len(slabs), per_level)
@@ -423,31 +485,36 @@ def serving_phase(capi, ctx, db_main, w, args, rank, loads=(0.5, 1.0, 1.5), seed
                 i, s = slabs[pick[k]]
                 tk.append(srv.submit(dbs[i], s, outs[(i, s)].data_ptr(), True))
             for t in tk:
-                srv.wait(t)
+                srv.wait(t, timeout_s=600.0)
             elapsed = time.perf_counter() - t_start
             st = srv.stats()
+            runs = [srv.info(t).run_ms for t in tk]
             levels.append({"load": load, "rate_per_s": rate, "requests": per_level,
                            "p50_ms": st.p50_ms, "p99_ms": st.p99_ms, "mean_ms": st.mean_ms,
-                           "queue_p99_ms": st.queue_p99_ms, "pairs_per_s": st.pairs / elapsed,
+                           "queue_p50_ms": st.queue_p50_ms, "queue_p99_ms": st.queue_p99_ms,
+                           "run_p50_ms": percentile(runs, 50), "run_p99_ms": percentile(runs, 99),
+                           "pairs_per_s": st.pairs / elapsed,
                            "max_concurrent": st.max_concurrent})
-    for d in own:
+    for d in dbs:
         d.close()
-    return {"boxes": names, "capacity_slabs_per_s": cap, "levels": levels}
+    return {"boxes": names, "slots": args.serve_slots, "capacity_slabs_per_s": cap,
+            "levels": levels}
 
 
-def precision_study(capi, box, w, device, stream, steps, comp_out, frac=1e-3, seed=11):
+def precision_study(capi, box, w, device, stream, steps, comp_out, variant, frac=1e-3, seed=11):
     """Compensated vs plain FP32 accumulation on the same box: the plain
-    form's sweep rate (device time, positions resident) and both results'
-    RMS / max fractional error against the FP64 oracle on a seeded subsample
-    of `frac` of the sinks.  `comp_out` is the compensated sweep's result."""
+    form's sweep rate (device time, positions resident, the compensated
+    sweep's kernel shape) and both results' RMS / max fractional error against
+    the FP64 oracle on a seeded subsample of `frac` of the sinks.  `comp_out`
+    is the compensated sweep's result."""
     import torch
     soft, eps = w["softening"], kernel_eps(w)
-    ctx = capi.Context(softening=soft, eps=eps, device=device, accumulation=capi.ACC_PLAIN)
+    ctx = capi.Context(softening=soft, eps=eps, device=device, accumulation=capi.ACC_PLAIN,
+                       kernel_variant=variant)
     ctx.set_stream(stream.cuda_stream)
     db = ctx.box(box)
     out = torch.empty((box.n, 4), dtype=torch.float32, device=f"cuda:{device}")
-    for _ in range(2):
-        db.forces_device(0, box.cpd, out.data_ptr())
+    db.forces_device(0, box.cpd, out.data_ptr())
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
@@ -458,8 +525,10 @@ def precision_study(capi, box, w, device, stream, steps, comp_out, frac=1e-3, se
     ms = e0.elapsed_time(e1) / steps
     pairs = db.pair_count()
     plain_out = out.cpu().numpy()
+    del out
     db.close()
     ctx.close()
+    torch.cuda.empty_cache()
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle
     k = max(2000, int(frac * box.n))
@@ -467,8 +536,8 @@ def precision_study(capi, box, w, device, stream, steps, comp_out, frac=1e-3, se
     t0 = time.perf_counter()
     ref = oracle.fp64_sinks(box, soft, eps, sinks)
     t_ref = time.perf_counter() - t0
-    res = {"sinks": k, "fp64_oracle_s": t_ref, "plain_pairs_per_s": pairs / (ms / 1e3),
-           "plain_ms_per_step": ms}
+    res = {"sinks": k, "fraction": k / box.n, "seed": seed, "fp64_oracle_s": t_ref,
+           "plain_pairs_per_s": pairs / (ms / 1e3), "plain_ms_per_step": ms, "plain_steps": steps}
     mag = np.linalg.norm(ref, axis=1)
     res["small_force_sinks"] = int((mag < 1e-3 * np.median(mag)).sum())  # |a64| < 1e-3 median
     for name, a in (("compensated", comp_out), ("plain", plain_out)):
@@ -477,45 +546,84 @@ def precision_study(capi, box, w, device, stream, steps, comp_out, frac=1e-3, se
     return res
 
 
+class Phases:
+    """Wall time of each bench phase (stderr as they end; kept for the line)."""
+
+    def __init__(self, rank):
+        self.rank = rank
+        self.t = {}
+
+    def run(self, name, fn, *a, **kw):
+        t0 = time.perf_counter()
+        r = fn(*a, **kw)
+        dt = time.perf_counter() - t0
+        self.t[name] = round(dt, 2)
+        if self.rank == 0:
+            print(f"[bench] {name}: {dt:.1f} s", file=sys.stderr, flush=True)
+        return r
+
+
+def fp32_peaks(ctx, clocks, sms):
+    """The FP32 roofline denominator: the paired-FMA probe (sustained) and the
+    clock-derived peak sms x 128 lanes x 2 flops x the median SM clock sampled
+    in the timed region; the larger of the two is used."""
+    burst, sust = ctx.fp32_peak(1.0)
+    mhz = clocks.get("sm_mhz") if isinstance(clocks, dict) else None
+    derived = sms * 128 * 2 * mhz * 1e6 / 1e12 if mhz else float("nan")
+    peak = max(sust, derived) if mhz else sust
+    src = ("clock-derived: %d SMs x 128 FP32 lanes x 2 flops x %.0f MHz (median SM clock "
+           "sampled in the timed region)" % (sms, mhz)) if mhz and derived >= sust else \
+        "paired-FMA probe on this GPU in this run, sustained over ~1 s"
+    return {"peak": peak, "peak_source": src, "peak_probe_sustained": sust,
+            "peak_probe_burst": burst, "peak_clock_derived": derived}
+
+
 def our_arm(args, w):
     import torch
     rank, world, local = dist_init(args.gpus)
     _pkg()
     from abacus_public_b200 import capi
-    box = make_box(w, seed_offset=rank_seed_offset(rank))
+    ph = Phases(rank)
+    box = ph.run("generate_box", make_box, w, seed_offset=rank_seed_offset(rank))
     eps = kernel_eps(w)
     soft = w["softening"]
     ctx = capi.Context(softening=soft, eps=eps, device=local)
     torch.cuda.set_device(local)
+    sms = torch.cuda.get_device_properties(local).multi_processor_count
     stream = torch.cuda.Stream(device=local)
     torch.cuda.set_stream(stream)
     ctx.set_stream(stream.cuda_stream)  # the library launches on the stream the events time
-    peak_burst, peak_sust = (float("nan"), float("nan")) if args.profile else ctx.fp32_peak(1.0)
-    db = ctx.box(box)
+    db = ph.run("upload", ctx.box, box)
     pairs = db.pair_count()
     n = box.n
     out_dev = torch.empty((n, 4), dtype=torch.float32, device=f"cuda:{local}")
-    # warm-up (graph capture happens on the first call)
-    for _ in range(args.warmup):
-        db.forces_device(0, box.cpd, out_dev.data_ptr())
-    torch.cuda.synchronize()
-    kernel_ms, step_ms_dev = [], []
-    with ClockSampler(local) as clk:
-        barrier(world)
+
+    def warm():
+        # the first call tunes the kernel shape and captures the graph
+        for _ in range(args.warmup):
+            db.forces_device(0, box.cpd, out_dev.data_ptr())
         torch.cuda.synchronize()
+    ph.run("tune_and_warmup", warm)
+    kernel_ms, step_ms_dev = [], []
+
+    def timed():
+        clk = ClockSampler(local)
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(args.steps):
-            db.forces_device(0, box.cpd, out_dev.data_ptr())
-            t = ctx.last_timing()
-            kernel_ms.append(t.kernel_ms)
-            step_ms_dev.append(t.total_ms)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        barrier(world)
-        elapsed = e0.elapsed_time(e1)
-    clocks = clk.summary()
+        with clk:
+            barrier(world)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            for _ in range(args.steps):
+                db.forces_device(0, box.cpd, out_dev.data_ptr())
+                t = ctx.last_timing()
+                kernel_ms.append(t.kernel_ms)
+                step_ms_dev.append(t.total_ms)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            barrier(world)
+        return e0.elapsed_time(e1), clk.summary(), t
+    elapsed, clocks, t = ph.run("timed_sweeps", timed)
     elapsed = barrier_max(elapsed, world)
     ms_per_step = elapsed / args.steps
     total_pairs = all_sum(float(pairs), world)
@@ -523,7 +631,6 @@ def our_arm(args, w):
     launches = args.steps * t.launches
 
     if args.profile:
-        t = ctx.last_timing()
         if rank == 0:
             print(json.dumps({"profile_run": args.workload, "ms_per_step": ms_per_step,
                               "kernel_ms": float(np.mean(kernel_ms)), "pairs": pairs,
@@ -531,6 +638,7 @@ def our_arm(args, w):
         db.close()
         ctx.close()
         return 0
+    peaks = ph.run("fp32_peak", fp32_peaks, ctx, clocks, sms)
     # end to end through the C ABI with pinned host buffers: H2D positions,
     # sweep, D2H accelerations, every step
     hx = torch.from_numpy(box.x).pin_memory()
@@ -538,34 +646,46 @@ def our_arm(args, w):
     hz = torch.from_numpy(box.z).pin_memory()
     hout = torch.empty((n, 4), dtype=torch.float32).pin_memory()
     xa, ya, za, oa = hx.numpy(), hy.numpy(), hz.numpy(), hout.numpy()
-    # one call per step: copies in, sweeps and copies out overlap over 8 slab
-    # chunks (nf_box_step); the first call builds the chunk plans
-    db.step(xa, ya, za, oa)
-    barrier(world)
-    torch.cuda.synchronize()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        db.step(xa, ya, za, oa)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    e2e_ms = barrier_max(e0.elapsed_time(e1) / args.steps, world)
-    e2e_value = total_pairs / (e2e_ms / 1e3)
+    e2e_steps = args.e2e_steps or args.steps
 
-    # the plain drop-in on the same box: NearFieldDriver -> SICs from host slabs
-    plain = None if args.no_plain else plain_dropin(capi, box, w, local, steps=2)
-    # serving: seeded Poisson slab requests over this box and a second one
-    serving = None if args.no_serving else serving_phase(capi, ctx, db, w, args, rank)
+    def e2e():
+        # one call per step: copies in, sweeps and copies out overlap over 8
+        # slab chunks (nf_box_step); the first call builds the chunk plans
+        db.step(xa, ya, za, oa)
+        barrier(world)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(e2e_steps):
+            db.step(xa, ya, za, oa)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / e2e_steps
+    e2e_ms = barrier_max(ph.run("e2e", e2e), world)
+    e2e_value = total_pairs / (e2e_ms / 1e3)
+    tv, tms = db.tuning()
+    db.close()
+    del out_dev
+    torch.cuda.empty_cache()
+
+    precision = plain = refk = None
+    if rank == 0 and not args.no_precision:
+        precision = ph.run("precision_study", precision_study, capi, box, w, local, stream,
+                           args.precision_steps, oa, tv)
+    if rank == 0 and not args.no_plain:
+        plain = ph.run("plain_dropin", plain_dropin, capi, box, w, local, a_batched=oa)
+        plain["batched_over_plain"] = e2e_value / plain["value"]
+        plain["batched_over_plain_what"] = "e2e (nf_box_step from pinned host buffers) over " \
+                                           "the drop-in's wall clock, same box"
+    if rank == 0 and not args.no_ref_kernel:
+        refk = ph.run("reference_gpu_kernel", ref_gpu_leg, box, w, oa)
+    serving = None if args.no_serving else ph.run("serving", serving_phase, capi, ctx, w, args,
+                                                  rank)
     # slab latency at half the measured closed-loop capacity (at 1.0x the
     # queue, not the device, sets the latency; every level is in "serving")
     lvl1 = None if serving is None else [v for v in serving["levels"] if v["load"] == 0.5][0]
-    # compensated vs plain accumulation against the FP64 oracle (0.1% of the sinks)
-    precision = None
-    if args.precision_study and rank == 0:
-        precision = precision_study(capi, box, w, local, stream, args.steps, oa)
 
-    tv, tms = db.tuning()
     lib = capi.lib()
     tune_info = {"variant": tv, "shape": lib.nf_kernel_variant_name(tv).decode(),
                  "candidates_ms": {lib.nf_kernel_variant_name(i).decode(): round(m, 3)
@@ -593,37 +713,46 @@ def our_arm(args, w):
                    "parallelism": f"independent boxes x{world}"},
         "slab_latency_ms": None if lvl1 is None else {
             "p50": lvl1["p50_ms"], "p99": lvl1["p99_ms"], "n": lvl1["requests"],
-            "what": "serving at 0.5x measured capacity: Poisson slab requests over two "
+            "queue_p99": lvl1["queue_p99_ms"], "run_p99": lvl1["run_p99_ms"],
+            "what": "serving at 0.5x measured capacity: Poisson slab requests over the "
                     "resident boxes, submit to result in the caller's device buffer"},
         "serving": serving,
         "precision": precision,
         "plain_dropin": plain,
-        "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak_sust, "unit": "TFLOP/s",
-                     "frac": achieved / peak_sust, "traffic": traffic,
+        "ref_gpu_kernel": refk,
+        "roofline": {"bound": "fp32", "achieved": achieved, "peak": peaks["peak"],
+                     "unit": "TFLOP/s", "frac": achieved / peaks["peak"], "traffic": traffic,
                      "kernel": "pencil_kernel", "kernel_ms": k_ms,
-                     "flops_per_pair": flops,
-                     "peak_source": "FFMA microbenchmark on this GPU in this run, sustained "
-                                    "(MEASURED_PEAKS.json has no FP32 figure)",
-                     "peak_burst": peak_burst,
+                     "flops_per_pair": flops, "peak_source": peaks["peak_source"],
+                     "peak_probe_sustained": peaks["peak_probe_sustained"],
+                     "peak_probe_burst": peaks["peak_probe_burst"],
+                     "peak_clock_derived": peaks["peak_clock_derived"],
                      "staging_hbm": staging_hbm(n, box_nc(w), k_ms, traffic)},
         "e2e": {"value": e2e_value, "unit": "pairs/s", "ms_per_step": e2e_ms,
+                "steps": e2e_steps,
                 "h2d_bytes_per_step": int(12 * n), "d2h_bytes_per_step": int(16 * n)},
         "gpu_launches": int(launches),
         "clocks": clocks,
         "autotune": tune_info,
     }
+    if precision is not None:
+        result["accuracy_vs_fp64"] = {"rms_frac": precision["compensated"]["rms_frac"],
+                                      "max_frac": precision["compensated"]["max_frac"],
+                                      "sinks": precision["sinks"]}
     if rank == 0 and not args.no_cpu_baseline:
-        rate, threads, desc, kind, _, _ = cpu_reference_rate(box, w, target_s=args.cpu_seconds)
-        result["cpu_baseline"] = {"value": rate, "unit": "pairs/s", "cores": threads,
-                                  "kind": kind, "sample": desc}
-        # precision of this run's result against the FP64 oracle (checker)
         sys.path.insert(0, str(ROOT / "oracle"))
         import oracle
-        a = oa  # the last full sweep, returned to the caller's host buffer
-        sinks = np.sort(np.random.default_rng(5).choice(n, 2000, replace=False))
-        rms, mx, _ = oracle.frac_errors(a[sinks, :3], oracle.fp64_sinks(box, soft, eps, sinks))
-        result["accuracy_vs_fp64"] = {"rms_frac": rms, "max_frac": mx, "sinks": 2000}
-    db.close()
+        threads = oracle.host_threads()
+        cells, sinks, spairs, desc = cpu_sample(box, args.cpu_pairs)
+        a_ref, dt, kind = ph.run("cpu_baseline", cpu_reference_run, box, w, cells, threads)
+        result["cpu_baseline"] = {"value": spairs / dt, "unit": "pairs/s", "cores": threads,
+                                  "kind": kind, "sample": f"{desc}, {dt:.1f} s"}
+        result["parity_vs_reference"] = dict(
+            parity_vs_reference(oa, a_ref, sinks),
+            reference="the reference CPU direct (Direct::Execute, -Ofast build) on the "
+                      "cpu_baseline sample",
+            ours="the last end-to-end sweep's output (nf_box_step)")
+    result["phase_s"] = ph.t
     ctx.close()
     if rank == 0:
         print(json.dumps(result), flush=True)
@@ -889,27 +1018,35 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="clustered256")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="clustered512")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--cpu-pairs", type=float, default=1.2e10,
+                    help="pairs in the fixed seeded row sample of the CPU reference (both arms)")
+    ap.add_argument("--e2e-steps", type=int, default=0,
+                    help="timed end-to-end steps (0: --steps)")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain drop-in phase")
-    ap.add_argument("--serve-requests", type=int, default=2000,
-                    help="slab requests per serving load level")
+    ap.add_argument("--no-ref-kernel", action="store_true",
+                    help="skip the reference GPU kernel leg")
+    ap.add_argument("--no-precision", action="store_true",
+                    help="skip the compensated-vs-plain precision study")
+    ap.add_argument("--precision-steps", type=int, default=3,
+                    help="timed sweeps of the plain-accumulation form")
+    ap.add_argument("--serve-requests", type=int, default=3000,
+                    help="slab requests per serving load level (half of it at 1.5x)")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving phase")
-    ap.add_argument("--serve-boxes", default="",
-                    help="serve clustered boxes of N=64*cpd^3 for these cpds (comma list) "
-                         "instead of the main box + a cpd-45 box")
-    ap.add_argument("--precision-study", action="store_true",
-                    help="also sweep with plain FP32 accumulation and compare both with the "
-                         "FP64 oracle on 0.1%% of the sinks")
+    ap.add_argument("--serve-boxes", default="45,65,85,105,125",
+                    help="serve clustered boxes of N=64*cpd^3 for these cpds (comma list)")
+    ap.add_argument("--serve-slots", type=int, default=8, help="serving slots (max_inflight)")
     ap.add_argument("--slabs", type=int, default=32,
                     help="clustered1024: the slab range [0, SLABS) a step sweeps (with "
                          "--full: slabs per launch)")
     ap.add_argument("--full", action="store_true",
                     help="clustered1024: one full sweep of the box, compensated and plain")
+    ap.add_argument("--replicas", action="store_true",
+                    help="with N > 1: one independent box per rank (weak scaling) instead of "
+                         "one box split over the ranks")
     ap.add_argument("--shard", action="store_true",
-                    help="split one box over the ranks (strong scaling, 2-slab halo exchange) "
-                         "instead of one independent box per rank")
+                    help="split one box over the ranks even at N = 1")
     ap.add_argument("--profile", action="store_true",
                     help="timed sweeps only (no peak probe, CPU baseline, e2e or latency "
                          "phases): the command profiled under ncu")
@@ -917,9 +1054,10 @@ def main():
     if args.warmup < 3:
         args.warmup = 3
     w = WORKLOADS[args.workload]
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     if args.impl == "reference":
         return reference_arm(args, w)
-    if args.shard:
+    if args.shard or (world > 1 and not args.replicas):
         return shard_arm(args, w)
     if w["kind"] == "clustered_device":
         return big_arm(args, w)

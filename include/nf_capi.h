@@ -191,6 +191,15 @@ nf_status nf_sic_execute(nf_ctx *ctx, const nf_sic_desc *sic, int jlow, int jhig
                          int blocking, volatile int *completion);
 /* Wait for every queued SIC (bounded). */
 nf_status nf_sic_drain(nf_ctx *ctx, uint64_t timeout_ns);
+/* Pencil-kernel time of the SICs completed on this context since the last
+ * reset (CUDA events around each SIC's launch, summed), how many SICs and
+ * their unpadded pairs; reset != 0 zeroes the counters after reading.  The
+ * reference times the same span per SIC with its DeviceData timers
+ * (PencilTask.cu:154-257, SetInteractionCollection.hh:243-248).  SICs that
+ * run concurrently on several buffers overlap, so their summed kernel time
+ * exceeds the wall time the GPU was busy. */
+nf_status nf_sic_timing(nf_ctx *ctx, double *kernel_ms, uint64_t *sics, uint64_t *pairs,
+                        int reset);
 
 /* ---------------- 2b. NearFieldDriver and the SIC planner ---------------- */
 /* The host side of the drop-in: a C++ NearFieldDriver with the reference's
@@ -490,7 +499,8 @@ nf_status nf_forces_noalloc(const nf_config *cfg, int cpd, const void *pos,
 nf_status nf_set_stream(nf_ctx *ctx, void *stream);
 
 /* FP32 roofline denominator measured on this device: a pure FFMA kernel
- * (8 independent chains per thread, every SM full) timed with CUDA events.
+ * (8 independent chains of paired f32x2 FMAs per thread, every SM full)
+ * timed with CUDA events.
  * burst = best of short runs; sustained = back-to-back for ~seconds_sustained.
  * Results in TFLOP/s (FFMA = 2 flops). */
 nf_status nf_measure_fp32_peak(nf_ctx *ctx, double seconds_sustained, double *burst_tflops,

@@ -329,11 +329,12 @@ def sic_arrays(box, slab, R=2, node=None):
                            n_q=n_q, ilist=ilist, yoff=yoff, s_src=s_src, s_dst=s_dst, n_p=n_p)
 
 
-def _coadd(box, slab, a, acc):
-    """Each sink's 2R+1 pencil partials summed in float32, in pencil order."""
+def _coadd(box, slab, a, acc, nc=3):
+    """Each sink's 2R+1 pencil partials summed in float32, in pencil order
+    (the first nc components of the records)."""
     p0, p1 = box.slab_range(slab)
-    out = np.zeros((p1 - p0, 3), np.float32)
-    np.add.at(out, a.s_src - p0, acc[a.s_dst, :3])
+    out = np.zeros((p1 - p0, nc), np.float32)
+    np.add.at(out, a.s_src - p0, acc[a.s_dst, :nc])
     return out
 
 
@@ -354,20 +355,27 @@ def cpu_execute_slab(box, eps, slab, R=2, node=None):
     return _coadd(box, slab, a, acc)
 
 
-def ref_gpu_slab(box, softening, eps, slab, repeats=1, b2=0.0, R=2, node=None):
+def ref_gpu_slab(box, softening, eps, slab, repeats=1, b2=0.0, R=2, node=None, with_w=False):
     """The reference GPU kernel on one whole x-slab as one SIC (the arrays of
     sic_arrays; node: one node of a 2D z-split): returns (acc float32[n_slab,
-    3] in particle order, mean launch ms, DirectTotal pairs).  The y shift is
-    applied on the device; the five pencil partials of each sink are co-added
-    in float32."""
-    a = sic_arrays(box, slab, R, node)
+    3] in particle order -- [n_slab, 4] with the density sum w when with_w --,
+    mean launch ms, DirectTotal pairs).  The y shift is applied on the
+    device; the five pencil partials of each sink are co-added in float32."""
+    return ref_gpu_run(box, softening, eps, slab, sic_arrays(box, slab, R, node), repeats=repeats,
+                       b2=b2, with_w=with_w)
+
+
+def ref_gpu_run(box, softening, eps, slab, a, repeats=1, b2=0.0, with_w=False):
+    """ref_gpu_slab on arrays already laid out by sic_arrays (so that a caller
+    can lay out the next slab while this one runs)."""
     P, nblk, nslots, nsrc = a.P, a.nblk, a.nslots, a.nsrc
     sx, sy, sz, tx, ty, tz = a.sx, a.sy, a.sz, a.tx, a.ty, a.tz
     id_max, parent, q_start, n_q, ilist, yoff = a.id_max, a.parent, a.q_start, a.n_q, a.ilist, a.yoff
-    f32 = np.float32
     L = ref_gpu_lib(softening)
     nf4 = L.nfrefgpu_accstruct_floats()
-    acc = np.zeros((max(nslots, 1), nf4), f32)
+    if with_w and nf4 < 4:
+        raise ValueError("the reference kernel was built without COMPUTE_FOF_DENSITY")
+    acc = np.zeros((max(nslots, 1), nf4), np.float32)
     sink_xyz = np.ascontiguousarray(np.concatenate([sx, sy, sz]))
     src_xyz = np.ascontiguousarray(np.concatenate([tx, ty, tz]))
     q_start32 = q_start.astype(np.int32)
@@ -382,4 +390,4 @@ def ref_gpu_slab(box, softening, eps, slab, repeats=1, b2=0.0, R=2, node=None):
     if rc != 0:
         raise RuntimeError(f"reference GPU kernel failed: cudaError {rc}")
     pairs = int((a.n_p[:, None] * n_q[ilist]).sum())
-    return _coadd(box, slab, a, acc), ms.value, pairs
+    return _coadd(box, slab, a, acc, 4 if with_w else 3), ms.value, pairs

@@ -1,0 +1,61 @@
+"""Host-side pieces of bench.py that decide what is measured (no GPU)."""
+import importlib.util
+import pathlib
+
+import numpy as np
+
+ROOT = pathlib.Path(__file__).resolve().parents[1]
+
+
+def _bench():
+    spec = importlib.util.spec_from_file_location("bench_under_test", ROOT / "bench.py")
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def test_cell_pairs_sum_to_direct_total(synth, oracle):
+    bench = _bench()
+    box = synth.clustered_box(40000, 11, seed=3, n_clumps=20)
+    cp = bench.cell_pairs(box)
+    assert cp.shape == (11, 11, 11)
+    assert int(cp.sum()) == oracle.pair_count(box)
+
+
+def test_cpu_sample_is_whole_rows_and_fixed(synth, oracle):
+    bench = _bench()
+    box = synth.clustered_box(40000, 11, seed=3, n_clumps=20)
+    total = oracle.pair_count(box)
+    cells, sinks, pairs, desc = bench.cpu_sample(box, 0.2 * total)
+    c2, s2, p2, d2 = bench.cpu_sample(box, 0.2 * total)
+    assert np.array_equal(cells, c2) and np.array_equal(sinks, s2) and p2 == pairs and d2 == desc
+    assert 0.2 * total <= pairs < total
+    # the sample is made of whole (x, y) rows, and its pairs are those rows' pairs
+    rows = np.unique(cells // box.cpd)
+    cp = bench.cell_pairs(box).reshape(-1, box.cpd)
+    assert pairs == int(cp[rows].sum())
+    full = (rows[:, None] * box.cpd + np.arange(box.cpd)).ravel()
+    assert np.array_equal(np.sort(cells), full[box.counts[full] > 0])
+    # sinks are exactly the particles of those cells, in cell order
+    cs = box.cell_start
+    want = np.concatenate([np.arange(cs[c], cs[c + 1]) for c in cells])
+    assert np.array_equal(sinks, want)
+    # a target beyond the box takes every row
+    cells_all, _, p_all, _ = bench.cpu_sample(box, 10 * total)
+    assert p_all == total and cells_all.size == int((box.counts > 0).sum())
+
+
+def test_parity_vs_reference_bound(synth):
+    bench = _bench()
+    rng = np.random.default_rng(0)
+    ref = rng.normal(size=(100, 3)).astype(np.float32)
+    sinks = np.arange(0, 100, 2)
+    got = np.concatenate([ref, np.zeros((100, 1), np.float32)], axis=1)
+    r = bench.parity_vs_reference(got, ref, sinks)
+    assert r["pass"] and r["max_comp_rel"] == 0.0 and r["sinks"] == 50
+    got[4, 1] += 1e-3 * np.linalg.norm(ref[4])  # a sampled sink off by 1e-3 of |a|
+    r = bench.parity_vs_reference(got, ref, sinks)
+    assert not r["pass"] and abs(r["max_comp_rel"] - 1e-3) < 1e-5
+    got[4, 1] = ref[4, 1]
+    got[5, 1] += 1.0  # an unsampled sink does not count
+    assert bench.parity_vs_reference(got, ref, sinks)["pass"]
