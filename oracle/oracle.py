@@ -204,10 +204,99 @@ def rescale_and_kick(nacc, far, vel, counts, near_scale, rescale, kick1, kick2, 
     nz = counts > 0
     starts = np.concatenate([[0], np.cumsum(counts)[:-1]])[nz]
     n2 = (v1[:, 0] * v1[:, 0] + v1[:, 1] * v1[:, 1]) + v1[:, 2] * v1[:, 2]
-    stats[nz, 0] = np.add.reduceat(n2, starts) / counts[nz].astype(np.float32)
+    # each cell's sum in float32, particle by particle in order (the loop of
+    # KickCell without OpenMP SIMD): step k adds every cell's k-th particle
+    cnt = counts[nz]
+    acc2 = np.zeros(cnt.size, np.float32)
+    for k in range(int(cnt.max()) if cnt.size else 0):
+        live = cnt > k
+        acc2[live] += n2[starts[live] + k]
+    stats[nz, 0] = acc2 / cnt.astype(np.float32)
     stats[nz, 1] = np.maximum.reduceat(np.abs(v1).max(axis=1), starts)
     stats[nz, 2] = np.maximum.reduceat(np.abs(a).max(axis=1), starts)
     return np.concatenate([a, w[:, None]], axis=1), v2, stats
+
+
+def kick_constants(omega_m, omega_smooth, np_total, make_glass, softening_length_internal):
+    """The two float factors RescaleAndCoAddAcceleration forms
+    (singlestep/Timestep/kick.cpp:75-92), computed in double and rounded to
+    float as there: rescale = -3 (Omega_M - Omega_Smooth) / (8 pi np) (negated
+    for glass) and the single spline's inv_eps3 = 1 / L^3."""
+    import math
+    rescale = np.float32(-3.0 * (omega_m - omega_smooth) / (8.0 * math.pi * np_total))
+    if make_glass:
+        rescale = np.float32(rescale * np.float32(-1))
+    L = float(softening_length_internal)
+    inv_eps3 = np.float32(1.0 / (L * L * L))
+    return rescale, inv_eps3
+
+
+# ---------------------------------------------------------------------------
+# the reference's own kick (oracle/_ref/libnfref_kick_*.so: kick.cpp compiled
+# unmodified by the Makefile with its FLOAT3p1 / ThreeVector types)
+# ---------------------------------------------------------------------------
+
+def have_ref_kick(softening: int) -> bool:
+    return softening in _GPU_SOFT and (REF_DIR / f"libnfref_kick_{_GPU_SOFT[softening]}.so").exists()
+
+
+_kick_libs = {}
+
+
+def ref_kick_lib(softening: int):
+    if softening not in _kick_libs:
+        L = ctypes.CDLL(str(REF_DIR / f"libnfref_kick_{_GPU_SOFT[softening]}.so"))
+        L.nfrefkick_rescale.argtypes = [ctypes.c_int64, _f32p, _f32p, ctypes.c_double,
+                                        ctypes.c_double, ctypes.c_int64, ctypes.c_int,
+                                        ctypes.c_double, ctypes.c_float]
+        L.nfrefkick_rescale.restype = ctypes.c_int
+        L.nfrefkick_kick_slab.argtypes = [ctypes.c_int, _i64p, _f32p, _f32p, ctypes.c_float,
+                                          ctypes.c_float, _f32p, ctypes.c_void_p]
+        L.nfrefkick_kick_slab.restype = ctypes.c_int
+        L.nfrefkick_acc_floats.restype = ctypes.c_int
+        _kick_libs[softening] = L
+    return _kick_libs[softening]
+
+
+def ref_rescale_and_kick(softening, nacc, far, vel, counts, cpd, omega_m, omega_smooth, np_total,
+                         make_glass, softening_length_internal, kick1, kick2, b2=0.0):
+    """The reference's RescaleAndCoAddAcceleration then KickSlab (kick.cpp),
+    slab by slab, on particles in cell order; counts: particles per cell of
+    whole slabs (a multiple of cpd^2 cells).  Same returns as
+    rescale_and_kick: (acc (N, 4), velocities after both half kicks, per-cell
+    stats (ncell, 3)) plus the aux density each particle was given."""
+    L = ref_kick_lib(softening)
+    assert L.nfrefkick_acc_floats() == 4
+    nacc = np.asarray(nacc, np.float32)
+    n = len(nacc)
+    acc = np.zeros((n, 4), np.float32)
+    acc[:, :nacc.shape[1]] = nacc
+    far = np.ascontiguousarray(far, np.float32)
+    v = np.array(vel, np.float32, copy=True)
+    counts = np.asarray(counts, np.int64)
+    c2 = cpd * cpd
+    assert counts.size % c2 == 0 and counts.sum() == n
+    stats = np.zeros((counts.size, 3), np.float32)
+    dens = np.zeros(n, np.float32)
+    p = 0
+    for s in range(counts.size // c2):
+        cnt = counts[s * c2:(s + 1) * c2]
+        m = int(cnt.sum())
+        a_s = np.ascontiguousarray(acc[p:p + m])
+        f_s = np.ascontiguousarray(far[p:p + m])
+        _check(L.nfrefkick_rescale(m, a_s.reshape(-1), f_s.reshape(-1), omega_m, omega_smooth,
+                                   int(np_total), int(make_glass),
+                                   float(softening_length_internal), b2))
+        v_s = np.ascontiguousarray(v[p:p + m])
+        st = np.zeros((c2, 3), np.float32)
+        d_s = np.zeros(m, np.float32)
+        cs = np.concatenate([[0], np.cumsum(cnt)]).astype(np.int64)
+        _check(L.nfrefkick_kick_slab(cpd, cs, v_s.reshape(-1), a_s.reshape(-1), kick1, kick2,
+                                     st.reshape(-1), d_s.ctypes.data_as(ctypes.c_void_p)))
+        acc[p:p + m], v[p:p + m], dens[p:p + m] = a_s, v_s, d_s
+        stats[s * c2:(s + 1) * c2] = st
+        p += m
+    return acc, v, stats, dens
 
 
 # ---------------------------------------------------------------------------

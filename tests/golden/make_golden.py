@@ -1,4 +1,5 @@
-"""Generate the golden near-field vectors from the reference's own CPU kernel.
+"""Generate the golden near-field vectors from the reference's own CPU kernel,
+and the golden kick vectors from the reference's own kick.
 
     python tests/golden/make_golden.py
 
@@ -40,7 +41,41 @@ CASES = [
 ]
 
 
+# RescaleAndCoAddAcceleration + KickSlab (singlestep/Timestep/kick.cpp,
+# compiled unmodified into oracle/_ref/libnfref_kick_<softening>.so with the
+# density channel on) on seeded arrays: two slabs of cpd 5, up to 40
+# particles per cell, near accelerations with a density w, far accelerations
+# and velocities.
+KICK = dict(cpd=5, omega_m=0.3089, omega_smooth=0.0, np_total=256 ** 3, make_glass=0,
+            kick1=0.0131, kick2=0.0117, b2=2.5e-7)
+
+
+def kick_main():
+    for soft, sli in ((0, 1.0 / 256 / 40), (1, 2.15517 / 256 / 40)):
+        rng = np.random.default_rng(20 + soft)
+        cpd = KICK["cpd"]
+        counts = rng.integers(0, 41, size=2 * cpd * cpd)
+        n = int(counts.sum())
+        scale = 1e11 if soft == 1 else 1e4  # raw near output: single spline lacks eps^-3
+        nacc = np.zeros((n, 4), np.float32)
+        nacc[:, :3] = rng.standard_normal((n, 3)) / scale * 1e7
+        nacc[:, 3] = KICK["b2"] * (1 + 20 * rng.random(n))
+        far = (rng.standard_normal((n, 3)) * 1e7).astype(np.float32)
+        vel = (rng.standard_normal((n, 3)) * 1e-2).astype(np.float32)
+        acc, v, stats, dens = O.ref_rescale_and_kick(
+            soft, nacc, far, vel, counts, cpd, KICK["omega_m"], KICK["omega_smooth"],
+            KICK["np_total"], KICK["make_glass"], sli, np.float32(KICK["kick1"]),
+            np.float32(KICK["kick2"]), np.float32(KICK["b2"]))
+        out = HERE / f"kick_{O.SOFTENING_NAMES[soft]}.npz"
+        np.savez_compressed(out, softening=soft, cpd=cpd, counts=counts, nacc=nacc, far=far,
+                            vel=vel, softening_length_internal=sli,
+                            **{k: v_ for k, v_ in KICK.items() if k != "cpd"},
+                            acc_out=acc, vel_out=v, stats_out=stats, dens_out=dens)
+        print(out.name, n, "particles")
+
+
 def main():
+    kick_main()
     for name, mk, nside, slabs in CASES:
         box = mk()
         for soft in range(4):

@@ -27,14 +27,22 @@ def test_aos_upload_equals_soa(capi, synth, kbox):
     assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
 
 
-@pytest.mark.parametrize("softening", [0, 1])
-def test_kick_matches_sweep_plus_reference_kick(capi, synth, oracle, kbox, softening):
+@pytest.mark.parametrize("softening,dens", [(0, False), (1, False), (1, True)])
+def test_kick_matches_sweep_plus_reference_kick(capi, synth, oracle, kbox, softening, dens):
+    """nf_box_kick against the sweep followed by the oracle's restatement of
+    kick.cpp and, where it is built, by the reference's own kick.cpp
+    (RescaleAndCoAddAcceleration + KickSlab, compiled unmodified): a, w and
+    v bit for bit, the cell maxima exactly, the mean square velocity to
+    1e-5 (summation order)."""
     import torch
     lo, hi = 3, 11
-    eps = synth.kernel_eps(softening, synth.plummer_eps(41))
-    L_int = synth.plummer_eps(41) * (synth.SINGLE_SPLINE_FACTOR if softening == 1 else 1.0)
-    near_scale = np.float32(1.0 / L_int ** 3) if softening == 1 else np.float32(1.0)
-    rescale = np.float32(-3.0 * (0.31 - 0.0) / (8.0 * np.pi * kbox.n))
+    length = synth.plummer_eps(41)
+    eps = synth.kernel_eps(softening, length)
+    L_int = length * (synth.SINGLE_SPLINE_FACTOR if softening == 1 else 1.0)
+    cosmo = (0.31, 0.0, kbox.n, 0, L_int)  # Omega_M, Omega_Smooth, np, MakeGlass, L
+    rescale, inv_eps3 = oracle.kick_constants(*cosmo)
+    near_scale = inv_eps3 if softening == 1 else np.float32(1.0)
+    b2 = np.float32((0.2 / kbox.cpd) ** 2) if dens else np.float32(0.0)
     k1, k2 = np.float32(0.013), np.float32(0.011)
     p0, p1 = kbox.slab_range(lo)[0], kbox.slab_range(hi - 1)[1]
     n = p1 - p0
@@ -43,9 +51,12 @@ def test_kick_matches_sweep_plus_reference_kick(capi, synth, oracle, kbox, softe
     vel = (rng.standard_normal((n, 3)) * 1e-2).astype(np.float32)
     c2 = kbox.cpd ** 2
     counts = kbox.counts[lo * c2:hi * c2]
-    with capi.Context(softening=softening, eps=eps) as ctx:
+    ref_kick = oracle.have_ref_kick(softening)
+    with capi.Context(softening=softening, eps=eps, b2=float(b2)) as ctx:
         db = ctx.box(kbox)
         nacc = db.forces(lo, hi)
+        if dens:
+            assert np.all(nacc[:, 3] >= b2 * (1 - 1e-6))
         d_far = torch.from_numpy(far).cuda()
         d_vel = torch.from_numpy(vel).cuda()
         d_acc = torch.empty((n, 4), dtype=torch.float32, device="cuda")
@@ -54,14 +65,18 @@ def test_kick_matches_sweep_plus_reference_kick(capi, synth, oracle, kbox, softe
             v_in = d_vel.cpu().numpy()
             db.kick(lo, hi, d_vel.data_ptr(), d_far.data_ptr(), d_acc.data_ptr(), d_st.data_ptr(),
                     near_scale=float(near_scale), rescale=float(rescale), kick1=float(k1),
-                    kick2=float(k2))
-            acc_w, v_w, st_w = oracle.rescale_and_kick(nacc, far, v_in, counts, near_scale,
-                                                       rescale, k1, k2)
-            assert np.array_equal(d_acc.cpu().numpy().view(np.uint32), acc_w.view(np.uint32))
-            assert np.array_equal(d_vel.cpu().numpy().view(np.uint32), v_w.view(np.uint32))
-            st = d_st.cpu().numpy()
-            assert np.array_equal(st[:, 1:], st_w[:, 1:])  # maxima: exact
-            np.testing.assert_allclose(st[:, 0], st_w[:, 0], rtol=1e-5, atol=0)
+                    kick2=float(k2), b2=float(b2))
+            got = (d_acc.cpu().numpy(), d_vel.cpu().numpy(), d_st.cpu().numpy())
+            wants = [oracle.rescale_and_kick(nacc, far, v_in, counts, near_scale, rescale, k1,
+                                             k2, b2=b2)]
+            if ref_kick:
+                wants.append(oracle.ref_rescale_and_kick(softening, nacc, far, v_in, counts,
+                                                         kbox.cpd, *cosmo, k1, k2, b2)[:3])
+            for acc_w, v_w, st_w in wants:
+                assert np.array_equal(got[0].view(np.uint32), acc_w.view(np.uint32))
+                assert np.array_equal(got[1].view(np.uint32), v_w.view(np.uint32))
+                assert np.array_equal(got[2][:, 1:], st_w[:, 1:])  # maxima: exact
+                np.testing.assert_allclose(got[2][:, 0], st_w[:, 0], rtol=1e-5, atol=0)
         db.close()
 
 

@@ -70,6 +70,64 @@ def test_2d_nodes_match_reference_gpu_kernel(capi, synth, oracle, softening):
                 float((diff[ok] / norm[ok, None]).max())
 
 
+def _check_xyzw(got, ref, b2, what):
+    """Forces within 1e-4 |a_ref| per component; the density sum w within
+    1e-5 relative (+1e-6 b2: pairs at r^2 ~ b^2 may fall either side)."""
+    r, g = ref.astype(np.float64), got.astype(np.float64)
+    norm = np.linalg.norm(r[:, :3], axis=1)
+    ok = norm > 0
+    diff = np.abs(g[:, :3] - r[:, :3])
+    assert np.all(diff[ok] <= 1e-4 * norm[ok, None]), (what, float((diff[ok] / norm[ok, None]).max()))
+    # every sink's own pair adds b2 (r = 0 < b), so w >= b2
+    assert np.all(r[:, 3] >= b2 * (1 - 1e-6)), what
+    np.testing.assert_allclose(g[:, 3], r[:, 3], rtol=1e-5, atol=1e-6 * b2, err_msg=what)
+
+
+@pytest.mark.parametrize("softening", [0, 1])
+def test_density_channel_matches_reference_gpu_kernel(capi, synth, oracle, softening):
+    """The FOF density channel (b2 > 0): the reference kernel's
+    direct_density (DirectGPUKernels.cuh, w += b2 - r^2 for r^2 < b2, built
+    with COMPUTE_FOF_DENSITY) against the batched sweep, the drop-in driver
+    and one node of a 2D z-split, x, y, z and w per sink."""
+    if not oracle.have_ref_gpu(softening):
+        pytest.skip("reference GPU kernel not built (needs the reference sources)")
+    box = synth.clustered_box(60000, 13, seed=73, n_clumps=20)
+    length = synth.plummer_eps(39)
+    eps = synth.kernel_eps(softening, length)
+    b2 = float(np.float32((0.2 / box.cpd) ** 2))  # a fifth of a cell width
+    with capi.Context(softening=softening, eps=eps, b2=b2) as ctx:
+        db = ctx.box(box)
+        got_box = db.forces()
+        db.close()
+    drv = capi.Driver(box, softening=softening, softening_length=length, b2=b2, direct_bpd=2)
+    try:
+        got_drv = drv.run_all()
+    finally:
+        drv.close()
+    zs, zn = 4, 5
+    drv = capi.Driver(box, softening=softening, softening_length=length, b2=b2, direct_bpd=2,
+                      node_z=(zs, zn))
+    try:
+        got_node = drv.run_all()
+    finally:
+        drv.close()
+    cpd = box.cpd
+    cellz = np.repeat(np.arange(cpd ** 3) % cpd, np.diff(box.cell_start))
+    multi = 0
+    for slab in (0, 6, 12):
+        p0, p1 = box.slab_range(slab)
+        ref, _, _ = oracle.ref_gpu_slab(box, softening, eps, slab, b2=b2, with_w=True)
+        assert ref.shape == (p1 - p0, 4)
+        multi += int((ref[:, 3] > 1.5 * b2).sum())  # sinks with neighbours inside b
+        _check_xyzw(got_box[p0:p1], ref, b2, f"batched slab {slab}")
+        _check_xyzw(got_drv[p0:p1], ref, b2, f"drop-in slab {slab}")
+        refn, _, _ = oracle.ref_gpu_slab(box, softening, eps, slab, b2=b2, with_w=True,
+                                         node=(zs, zn))
+        prim = (cellz[p0:p1] - zs) % cpd < zn
+        _check_xyzw(got_node[p0:p1][prim], refn[prim], b2, f"2D node slab {slab}")
+    assert multi > 1000
+
+
 def test_reference_kernel_bar(capi, synth, oracle):
     if not oracle.have_ref_gpu(1):
         pytest.skip("reference GPU kernel not built (needs the reference sources)")
