@@ -251,25 +251,25 @@ def cell_pairs(box, R=2):
 
 
 def cpu_sample(box, target_pairs, seed=CPU_SAMPLE_SEED):
-    """A fixed seeded sample for the CPU reference: whole (x, y) rows of cells
-    (the unit of ExecuteSlabCPU's loop over y, extras_directdriver.cpp:59-122)
-    in a seeded order until target_pairs is reached (the whole box if it holds
-    fewer).  Both bench arms take the same rows.  Returns (cells, sinks,
-    pairs, description)."""
-    cpd = box.cpd
-    rows = cell_pairs(box).sum(axis=2).ravel()  # row x*cpd + y
-    order = np.random.default_rng(seed).permutation(rows.size)
-    cum = np.cumsum(rows[order])
-    k = min(int(np.searchsorted(cum, target_pairs)) + 1, rows.size)
-    chosen = np.sort(order[:k])
-    cells = (chosen[:, None] * cpd + np.arange(cpd)[None, :]).ravel()
+    """A fixed seeded sample for the CPU reference: sink cells (the unit of
+    ExecuteSlabCPU's work, extras_directdriver.cpp:59-122) taken in a seeded
+    order of the non-empty cells until target_pairs is reached (the whole
+    box if it holds fewer), exact pair counts.  Cells and not whole rows or
+    slabs: on the clustered boxes one row through a clump holds ~3e10 pairs,
+    half a minute of the host's work.  Both bench arms take the same cells.
+    Returns (cells, sinks, pairs, description)."""
+    cp = cell_pairs(box).ravel()
+    nz = np.nonzero(box.counts)[0]
+    order = np.random.default_rng(seed).permutation(nz)
+    cum = np.cumsum(cp[order])
+    k = min(int(np.searchsorted(cum, target_pairs)) + 1, order.size)
+    cells = np.sort(order[:k])
     cs = box.cell_start
-    cells = cells[cs[cells + 1] > cs[cells]]
     n = (cs[cells + 1] - cs[cells]).astype(np.int64)
     sinks = np.repeat(cs[cells] - np.cumsum(n) + n, n) + np.arange(int(n.sum()))
-    pairs = int(rows[chosen].sum())
-    desc = (f"{k} seeded (x, y) rows of cells (seed {seed}; {cells.size} non-empty cells, "
-            f"{sinks.size} sinks, {pairs:.4e} pairs)")
+    pairs = int(cp[cells].sum())
+    desc = (f"{k} seeded non-empty sink cells (seed {seed}; {sinks.size} sinks, "
+            f"{pairs:.4e} pairs)")
     return cells, sinks, pairs, desc
 
 
@@ -397,12 +397,14 @@ def plain_dropin(capi, box, w, device, a_batched=None, steps=2):
     return res
 
 
-def ref_gpu_leg(box, w, a_batched):
+def ref_gpu_leg(box, w, a_batched, fp64=None):
     """The reference's own GPU kernel (ComputeDirects, PencilKernel.cu:97-188,
     compiled from its sources for sm_100a) on every x-slab of the box as one
     SIC, each laid out on the host as PencilOnPencil.cc / PencilPlan.cc do
     while the previous slab runs: pairs / summed launch time, and the largest
-    per-component deviation of its forces from the batched sweep's."""
+    per-component deviation of its forces from the batched sweep's.  fp64 =
+    (sinks, FP64 accelerations): the kernel's own error against the FP64
+    oracle on those sinks, beside the batched sweep's."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle
     from concurrent.futures import ThreadPoolExecutor
@@ -410,6 +412,7 @@ def ref_gpu_leg(box, w, a_batched):
     if not oracle.have_ref_gpu(soft):
         return {"unavailable": "the reference GPU kernel is not built for this softening"}
     tot_ms, pairs, worst = 0.0, 0, 0.0
+    mine = None if fp64 is None else np.zeros((fp64[0].size, 3), np.float32)
     with ThreadPoolExecutor(1) as ex:
         fut = ex.submit(oracle.sic_arrays, box, 0)
         for s in range(box.cpd):
@@ -421,14 +424,22 @@ def ref_gpu_leg(box, w, a_batched):
             tot_ms += ms
             pairs += p
             p0, p1 = box.slab_range(s)
+            if mine is not None:
+                sel = (fp64[0] >= p0) & (fp64[0] < p1)
+                mine[sel] = acc[fp64[0][sel] - p0]
             ref = acc.astype(np.float64)
             norm = np.linalg.norm(ref, axis=1)
             ok = norm > 0
             if ok.any():
                 dev = np.abs(np.asarray(a_batched[p0:p1, :3], np.float64) - ref).max(axis=1)
                 worst = max(worst, float((dev[ok] / norm[ok]).max()))
+    out = {}
+    if mine is not None:
+        rms, mx, _ = oracle.frac_errors(mine, fp64[1])
+        out = {"vs_fp64": {"rms_frac": rms, "max_frac": mx, "sinks": int(fp64[0].size),
+                           "what": "its own error on the precision study's FP64 sinks"}}
     return {"value": pairs / (tot_ms / 1e3), "unit": "pairs/s", "kernel_ms": tot_ms,
-            "pairs": pairs, "sics": box.cpd, "max_comp_rel_vs_batched": worst,
+            "pairs": pairs, "sics": box.cpd, "max_comp_rel_vs_batched": worst, **out,
             "what": "reference ComputeDirects (PencilKernel.cu) built for sm_100a with its "
                     "default GPU flags, one SIC per x-slab, summed CUDA-event launch time"}
 
@@ -543,7 +554,7 @@ def precision_study(capi, box, w, device, stream, steps, comp_out, variant, frac
     for name, a in (("compensated", comp_out), ("plain", plain_out)):
         rms, mx, _ = oracle.frac_errors(a[sinks, :3], ref)
         res[name] = {"rms_frac": rms, "max_frac": mx}
-    return res
+    return res, (sinks, ref)
 
 
 class Phases:
@@ -669,17 +680,17 @@ def our_arm(args, w):
     del out_dev
     torch.cuda.empty_cache()
 
-    precision = plain = refk = None
+    precision = plain = refk = fp64 = None
     if rank == 0 and not args.no_precision:
-        precision = ph.run("precision_study", precision_study, capi, box, w, local, stream,
-                           args.precision_steps, oa, tv)
+        precision, fp64 = ph.run("precision_study", precision_study, capi, box, w, local,
+                                 stream, args.precision_steps, oa, tv)
     if rank == 0 and not args.no_plain:
         plain = ph.run("plain_dropin", plain_dropin, capi, box, w, local, a_batched=oa)
         plain["batched_over_plain"] = e2e_value / plain["value"]
         plain["batched_over_plain_what"] = "e2e (nf_box_step from pinned host buffers) over " \
                                            "the drop-in's wall clock, same box"
     if rank == 0 and not args.no_ref_kernel:
-        refk = ph.run("reference_gpu_kernel", ref_gpu_leg, box, w, oa)
+        refk = ph.run("reference_gpu_kernel", ref_gpu_leg, box, w, oa, fp64)
     serving = None if args.no_serving else ph.run("serving", serving_phase, capi, ctx, w, args,
                                                   rank)
     # slab latency at half the measured closed-loop capacity (at 1.0x the

@@ -22,7 +22,7 @@ def test_cell_pairs_sum_to_direct_total(synth, oracle):
     assert int(cp.sum()) == oracle.pair_count(box)
 
 
-def test_cpu_sample_is_whole_rows_and_fixed(synth, oracle):
+def test_cpu_sample_is_fixed_and_exact(synth, oracle):
     bench = _bench()
     box = synth.clustered_box(40000, 11, seed=3, n_clumps=20)
     total = oracle.pair_count(box)
@@ -30,17 +30,14 @@ def test_cpu_sample_is_whole_rows_and_fixed(synth, oracle):
     c2, s2, p2, d2 = bench.cpu_sample(box, 0.2 * total)
     assert np.array_equal(cells, c2) and np.array_equal(sinks, s2) and p2 == pairs and d2 == desc
     assert 0.2 * total <= pairs < total
-    # the sample is made of whole (x, y) rows, and its pairs are those rows' pairs
-    rows = np.unique(cells // box.cpd)
-    cp = bench.cell_pairs(box).reshape(-1, box.cpd)
-    assert pairs == int(cp[rows].sum())
-    full = (rows[:, None] * box.cpd + np.arange(box.cpd)).ravel()
-    assert np.array_equal(np.sort(cells), full[box.counts[full] > 0])
+    # non-empty cells, sorted, and their exact pairs
+    assert np.all(np.diff(cells) > 0) and np.all(box.counts[cells] > 0)
+    assert pairs == int(bench.cell_pairs(box).ravel()[cells].sum())
     # sinks are exactly the particles of those cells, in cell order
     cs = box.cell_start
     want = np.concatenate([np.arange(cs[c], cs[c + 1]) for c in cells])
     assert np.array_equal(sinks, want)
-    # a target beyond the box takes every row
+    # a target beyond the box takes every non-empty cell
     cells_all, _, p_all, _ = bench.cpu_sample(box, 10 * total)
     assert p_all == total and cells_all.size == int((box.counts > 0).sum())
 
