@@ -240,16 +240,21 @@ __device__ __forceinline__ int64_t sink_particle(const WarpSmem &ws, int i, int 
     return ws.sstart[a] + (i - ws.spre[a]);
 }
 
-// Fold a partial p into the running (hi, lo) TwoSum pair (plain: one FP32
-// running sum) and clear it.  Scalar and paired (two sinks) forms; a - b is
-// formed as fma(b, -1, a), which rounds exactly like a subtraction.
+// Fold a partial p into the running compensated sum (h, l) and clear it
+// (plain: one FP32 running sum).  Kahan's compensated summation with the
+// correction kept as the low part to add (the sum is h + l):
+//   y = p + l;  t = h + y;  l = y - (t - h);  h = t
+// four paired instructions per component and sink pair.  Scalar and paired
+// (two sinks) forms; a - b is formed as fma(b, -1, a), which rounds exactly
+// like a subtraction.
 __device__ __forceinline__ void fold1(float &h, float &l, float &p, bool plain) {
     if (plain) {
         h += p;
     } else {
-        float e;
-        two_sum(h, p, h, e);
-        l += e;
+        float y = p + l;
+        float t = h + y;
+        l = y - (t - h);
+        h = t;
     }
     p = 0.f;
 }
@@ -259,17 +264,15 @@ __device__ __forceinline__ void fold2(float2 &h, float2 &l, float2 &p, bool plai
         h = add2(h, p);
     } else {
         const float2 m1 = dup2(-1.0f);
-        float2 s = add2(h, p);
-        float2 bb = fma2(h, m1, s);                  // s - h
-        float2 ea = fma2(fma2(bb, m1, s), m1, h);    // h - (s - bb)
-        float2 eb = fma2(bb, m1, p);                 // p - bb
-        l = add2(l, add2(ea, eb));
-        h = s;
+        float2 y = add2(p, l);
+        float2 t = add2(h, y);
+        l = fma2(fma2(h, m1, t), m1, y);  // y - (t - h)
+        h = t;
     }
     p = make_float2(0.f, 0.f);
 }
 
-// FP32 partials are folded into the (hi, lo) pairs every FOLD_CHUNKS chunks.
+// FP32 partials are folded into the compensated (h, l) sums every FOLD_CHUNKS chunks.
 constexpr int FOLD_CHUNKS = 2;
 
 template <int SOFT, bool DENS, int S, int UNR>

@@ -72,7 +72,10 @@ def test_2d_nodes_match_reference_gpu_kernel(capi, synth, oracle, softening):
 
 def _check_xyzw(got, ref, b2, what):
     """Forces within 1e-4 |a_ref| per component; the density sum w within
-    1e-5 relative (+1e-6 b2: pairs at r^2 ~ b^2 may fall either side)."""
+    1e-4 relative as well: both sides add w as one plain FP32 running sum per
+    pencil over up to thousands of terms (the reference kernel's a.w,
+    PencilKernel.cu:115-183), whose own rounding reaches a few 1e-5 in the
+    clumps."""
     r, g = ref.astype(np.float64), got.astype(np.float64)
     norm = np.linalg.norm(r[:, :3], axis=1)
     ok = norm > 0
@@ -80,7 +83,7 @@ def _check_xyzw(got, ref, b2, what):
     assert np.all(diff[ok] <= 1e-4 * norm[ok, None]), (what, float((diff[ok] / norm[ok, None]).max()))
     # every sink's own pair adds b2 (r = 0 < b), so w >= b2
     assert np.all(r[:, 3] >= b2 * (1 - 1e-6)), what
-    np.testing.assert_allclose(g[:, 3], r[:, 3], rtol=1e-5, atol=1e-6 * b2, err_msg=what)
+    np.testing.assert_allclose(g[:, 3], r[:, 3], rtol=1e-4, atol=0, err_msg=what)
 
 
 @pytest.mark.parametrize("softening", [0, 1])
@@ -125,6 +128,12 @@ def test_density_channel_matches_reference_gpu_kernel(capi, synth, oracle, softe
                                          node=(zs, zn))
         prim = (cellz[p0:p1] - zs) % cpd < zn
         _check_xyzw(got_node[p0:p1][prim], refn[prim], b2, f"2D node slab {slab}")
+        # both against the FP64 density sum: ours is no worse than the reference's
+        sinks = np.arange(p0, p1, 7)
+        w64 = oracle.fp64_density(box, b2, sinks)
+        e_ours = np.abs(got_box[sinks, 3] - w64) / w64
+        e_ref = np.abs(ref[sinks - p0, 3] - w64) / w64
+        assert e_ours.max() <= 1e-4 and np.sqrt(np.mean(e_ours ** 2)) <= 2 * np.sqrt(np.mean(e_ref ** 2)) + 1e-7
     assert multi > 1000
 
 
