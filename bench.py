@@ -479,6 +479,13 @@ def serving_phase(capi, ctx, w, args, rank, seed=7):
             for t in tk:
                 srv.wait(t, timeout_s=600.0)
             cap = len(slabs) / (time.perf_counter() - t0)
+        # each slab alone on the GPU once: the service times the workload
+        # itself sets (a floor under any request's latency)
+        solo = []
+        for i, s in slabs:
+            t = srv.submit(dbs[i], s, outs[(i, s)].data_ptr(), True)
+            srv.wait(t, timeout_s=600.0)
+            solo.append(srv.info(t).run_ms)
         for load, per_level in ((0.5, n_req), (1.0, n_req), (1.5, max(n_req // 2, 1))):
             rate = load * cap
             arr = np.cumsum(rng.exponential(1.0 / rate, per_level))
@@ -508,7 +515,11 @@ def serving_phase(capi, ctx, w, args, rank, seed=7):
                            "max_concurrent": st.max_concurrent})
     for d in dbs:
         d.close()
+    p50, p99 = percentile(solo, 50), percentile(solo, 99)
     return {"boxes": names, "slots": args.serve_slots, "capacity_slabs_per_s": cap,
+            "solo_service_ms": {"p50": p50, "p99": p99, "p99_over_p50": p99 / p50,
+                                "what": "each slab alone on the GPU, admission to result "
+                                        "(uniform over the boxes' slabs, as the requests)"},
             "levels": levels}
 
 
@@ -994,7 +1005,9 @@ def shard_arm(args, w):
     e2e_ms = barrier_max(e0.elapsed_time(e1) / args.steps, world)
     nbytes = all_sum(float(sum(v.numel() * 4 for v in host.values())), world)
     flops = FLOPS_PER_PAIR[w["softening"]]
-    peak_b, peak_s = ctx.fp32_peak(1.0)
+    clocks = clk.summary()
+    peaks = fp32_peaks(ctx, clocks, torch.cuda.get_device_properties(local).multi_processor_count)
+    peak_s = peaks["peak"]
     achieved = pairs * flops / (k_ms / 1e3) / 1e12
     result = {
         "metric": "pair_interactions_per_s", "value": total_pairs / (ms / 1e3), "unit": "pairs/s",
@@ -1006,12 +1019,13 @@ def shard_arm(args, w):
                    "slabs": parts, "l2": "inputs larger than L2"},
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak_s, "unit": "TFLOP/s",
                      "frac": achieved / peak_s, "traffic": None, "kernel": "pencil_kernel",
-                     "kernel_ms": k_ms, "note": "slowest rank's kernel time, its own pairs"},
+                     "kernel_ms": k_ms, "note": "slowest rank's kernel time, its own pairs",
+                     "peak_source": peaks["peak_source"]},
         "e2e": {"value": total_pairs / (e2e_ms / 1e3), "unit": "pairs/s", "ms_per_step": e2e_ms,
                 "h2d_bytes_per_step": int(nbytes), "d2h_bytes_per_step": int(16 * (p1 - p0) * world)},
         # per step: the sweep's launches, plus order_keys and pack_ordered of the upload
         "gpu_launches": int(args.steps * (ctx.last_timing().launches + 2)),
-        "clocks": clk.summary(),
+        "clocks": clocks,
     }
     db.close()
     ctx.close()
