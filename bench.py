@@ -306,6 +306,15 @@ def parity_vs_reference(a_gpu, a_ref, sinks, tol=1e-4):
             "pass": bool(np.all(dev <= tol * norm))}
 
 
+def workload_config(args, w, box, pairs, world=1):
+    """The `config` of the bench line: the workload alone, identical in both
+    arms at N = 1."""
+    return {"workload": args.workload, "desc": w["desc"], "particles_per_gpu": int(box.n),
+            "cpd": int(box.cpd), "pairs_per_step_per_gpu": int(pairs),
+            "l2": "inputs larger than L2 (positions 16 B x N + 120 B x N partials)",
+            "parallelism": f"independent boxes x{world}"}
+
+
 def reference_arm(args, w):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -332,9 +341,9 @@ def reference_arm(args, w):
         "unit": "pairs/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic",
-        "config": {"workload": args.workload, "desc": w["desc"],
-                   "step": "the reference CPU direct on a fixed seeded sample of whole rows "
-                           "of cells of the box (a whole sweep takes hours on the host)"},
+        "config": workload_config(args, w, box, int(cell_pairs(box).sum())),
+        "step": "the reference CPU direct on a fixed seeded sample of sink cells of the box "
+                "(a whole sweep takes hours on the host)",
         "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": threads, "kind": kind,
                          "sample": desc},
         "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0,
@@ -727,12 +736,9 @@ def our_arm(args, w):
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
-        "config": {"workload": args.workload, "desc": w["desc"], "particles_per_gpu": n,
-                   "cpd": box.cpd, "pairs_per_step_per_gpu": pairs,
-                   "padded_pairs_per_step_per_gpu": int(t.padded_pairs),
-                   "accumulation": "compensated",
-                   "l2": "inputs larger than L2 (positions 16 B x N + 120 B x N partials)",
-                   "parallelism": f"independent boxes x{world}"},
+        "config": workload_config(args, w, box, pairs, world),
+        "padded_pairs_per_step_per_gpu": int(t.padded_pairs),
+        "accumulation": "compensated",
         "slab_latency_ms": None if lvl1 is None else {
             "p50": lvl1["p50_ms"], "p99": lvl1["p99_ms"], "n": lvl1["requests"],
             "queue_p99": lvl1["queue_p99_ms"], "run_p99": lvl1["run_p99_ms"],

@@ -83,6 +83,11 @@ def test_uniform_64_plummer_full_box(capi, oracle, synth):
     for s in range(box.cpd):
         oracle.ref32_slab(box, 0, eps, s, acc=ref)
     _check_vs_ref(a, ref)
+    # the thinnest margin of the parity bound in the suite: print it (-s)
+    norm = np.linalg.norm(ref.astype(np.float64), axis=1)
+    worst = float((np.abs(a[:, :3].astype(np.float64) - ref).max(axis=1) / norm).max())
+    print(f"\n[uniform 64^3 Plummer] worst per-component deviation from the reference "
+          f"CPU direct: {worst:.3e} of |a_ref| (bound {GOLDEN_TOL_COMP:g})")
     sinks = np.sort(np.random.default_rng(0).choice(box.n, 3000, replace=False))
     rms, mx, _ = oracle.frac_errors(a[sinks, :3], oracle.fp64_sinks(box, 0, eps, sinks))
     assert rms <= FP64_RMS and mx <= FP64_MAX, (rms, mx)
