@@ -598,7 +598,7 @@ class Driver:
 class Server:
     """nf_server: slab requests over resident boxes, continuous admission."""
 
-    def __init__(self, ctx: Context, hbm_budget_bytes: int = 0, max_inflight: int = 8,
+    def __init__(self, ctx: Context, hbm_budget_bytes: int = 0, max_inflight: int = 2,
                  max_queued: int = 65536):
         self.ctx = ctx
         cfg = ServerConfig(hbm_budget_bytes, max_inflight, max_queued)

@@ -352,7 +352,10 @@ extern "C" nf_status nf_server_start(nf_ctx *ctx, const nf_server_config *cfg, n
     auto s = std::make_unique<nf_server>();
     s->ctx = ctx;
     if (cfg) s->cfg = *cfg;
-    if (s->cfg.max_inflight <= 0) s->cfg.max_inflight = 8;
+    // two slots by default: one request running and the next already queued
+    // on the device behind it.  More slots overlap persistent launches that
+    // share the GPU, which stretches every request's run time.
+    if (s->cfg.max_inflight <= 0) s->cfg.max_inflight = 2;
     if (s->cfg.max_queued <= 0) s->cfg.max_queued = 65536;
     if (s->cfg.max_inflight > 256) {
         set_error("nf_server_start: max_inflight above 256");

@@ -1067,7 +1067,7 @@ def main():
     ap.add_argument("--no-serving", action="store_true", help="skip the serving phase")
     ap.add_argument("--serve-boxes", default="45,65,85,105,125",
                     help="serve clustered boxes of N=64*cpd^3 for these cpds (comma list)")
-    ap.add_argument("--serve-slots", type=int, default=8, help="serving slots (max_inflight)")
+    ap.add_argument("--serve-slots", type=int, default=2, help="serving slots (max_inflight)")
     ap.add_argument("--slabs", type=int, default=32,
                     help="clustered1024: the slab range [0, SLABS) a step sweeps (with "
                          "--full: slabs per launch)")

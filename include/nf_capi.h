@@ -398,7 +398,9 @@ typedef uint64_t nf_ticket;
 typedef struct nf_server_config {
     size_t hbm_budget_bytes;  /* device bytes admitted requests may hold; 0 = 90% of the
                                  device memory free when the server starts */
-    int max_inflight;         /* slots: requests on the device at once (default 8) */
+    int max_inflight;         /* slots: requests on the device at once (default 2: one
+                                 running, the next queued behind it; more slots overlap
+                                 requests that then share the GPU and all run longer) */
     int max_queued;           /* pending requests beyond which submit fails (default 65536) */
 } nf_server_config;
 
