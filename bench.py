@@ -465,11 +465,16 @@ def serving_phase(capi, ctx, w, args, rank, seed=7):
     soft = w["softening"]
     cpds = [int(c) for c in args.serve_boxes.split(",")]
     dbs, names = [], []
+    hosts, epss = [], []
     for k, c in enumerate(cpds):
         x, y, z, cs = synth.clustered_box_device(64 * c ** 3, c, seed=100 + 17 * k + rank)
         d = ctx.box(synth.Box(c, x, y, z, cs, f"serve cpd {c}"))
+        # a host copy for the FP64 check of the served results
+        hosts.append(synth.Box(c, x.cpu().numpy(), y.cpu().numpy(), z.cpu().numpy(), cs,
+                               f"serve cpd {c}"))
         del x, y, z
-        d.set_eps(synth.kernel_eps(soft, synth.plummer_eps(4 * c)))  # 64 per cell: spacing h/4
+        epss.append(synth.kernel_eps(soft, synth.plummer_eps(4 * c)))  # 64 per cell: spacing h/4
+        d.set_eps(epss[-1])
         dbs.append(d)
         names.append(f"64*{c}^3 cpd {c} clustered")
     torch.cuda.empty_cache()
@@ -522,6 +527,24 @@ def serving_phase(capi, ctx, w, args, rank, seed=7):
                            "run_p50_ms": percentile(runs, 50), "run_p99_ms": percentile(runs, 99),
                            "pairs_per_s": st.pairs / elapsed,
                            "max_concurrent": st.max_concurrent})
+    # accuracy of the served results (the last request of each slab wrote
+    # its buffer): 3 seeded slabs of every box, up to 200 seeded sinks each,
+    # against the FP64 oracle
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+    acc = {}
+    for i, d in enumerate(dbs):
+        r = np.random.default_rng(300 + i)
+        got, a64 = [], []
+        for s in r.choice(d.cpd, 3, replace=False):
+            p0, p1 = d.slab_particles(int(s), int(s) + 1)
+            if p1 - p0 == 0:
+                continue
+            loc = np.sort(r.choice(p1 - p0, min(200, p1 - p0), replace=False))
+            got.append(outs[(i, int(s))][torch.from_numpy(loc).cuda(), :3].cpu().numpy())
+            a64.append(oracle.fp64_sinks(hosts[i], soft, epss[i], loc + p0))
+        rms, mx, _ = oracle.frac_errors(np.concatenate(got), np.concatenate(a64))
+        acc[names[i]] = {"rms_frac": rms, "max_frac": mx, "sinks": int(sum(len(g) for g in got))}
     for d in dbs:
         d.close()
     p50, p99 = percentile(solo, 50), percentile(solo, 99)
@@ -529,6 +552,7 @@ def serving_phase(capi, ctx, w, args, rank, seed=7):
             "solo_service_ms": {"p50": p50, "p99": p99, "p99_over_p50": p99 / p50,
                                 "what": "each slab alone on the GPU, admission to result "
                                         "(uniform over the boxes' slabs, as the requests)"},
+            "accuracy_vs_fp64": acc,
             "levels": levels}
 
 
