@@ -90,6 +90,18 @@ def _worker(rank, world, port, q):
             np.array_equal(halo_t[s][0], want[s].counts)
             and np.array_equal(halo_t[s][1].numpy(), np.stack([want[s].x, want[s].y, want[s].z]))
             for s in want)
+        # the bench's sharded arm: ranges cut by pair count (at least R slabs
+        # each), the tensor exchange given those ranges
+        parts = shard.partition(box.cpd, world, weights=shard.slab_pairs(box), min_slabs=2)
+        plo, phi = parts[rank]
+        owned_w = {s: (d.counts, torch.from_numpy(np.stack([d.x, d.y, d.z])))
+                   for s, d in shard.extract(box, range(plo, phi)).items()}
+        halo_w = shard.exchange_device(owned_w, rank, world, box.cpd, parts=parts)
+        need = [s for s in shard.window_slabs(plo, phi, box.cpd) if not plo <= s < phi]
+        want_w = shard.extract(box, need)
+        ok = ok and sorted(halo_w) == sorted(want_w) and all(
+            np.array_equal(halo_w[s][1].numpy(), np.stack([want_w[s].x, want_w[s].y, want_w[s].z]))
+            for s in want_w)
         q.put((rank, ok, sorted(halo)))
     finally:
         dist.destroy_process_group()
