@@ -31,6 +31,7 @@ namespace nf {
 static_assert(ENGINE_WARPS_PER_CTA == 8, "engine CTA shape");
 
 constexpr int NFBLOCK = 64;    // NFBlockSize (configure.ac:160-162)
+constexpr int SPLIT_MIN_SOURCES = 64;  // sources per warp of a split tile (one staged chunk)
 constexpr int REF_WIDTH = 5;   // WIDTH = 2*NFRADIUS+1, NFRADIUS = 2 (GPUControl.cu:109-113)
 
 struct SicTask {
@@ -312,7 +313,39 @@ static nf_status run_task(nf_ctx *ctx, SicBuffer &b, const SicTask &t) {
     std::stable_sort(items.begin(), items.end(), [](const Item &a, const Item &b) {
         return (int64_t)a.nsink * a.src_end > (int64_t)b.nsink * b.src_end;
     });
-    nitems = items.size();
+    // A SIC with fewer tiles than the launch has warps (small boxes, thin
+    // y-splits) would leave most of the GPU idle: then every tile with at
+    // least 64 sources per warp is split over the 8 warps of a CTA along its
+    // source stream (summed in warp order in shared memory), the engine's
+    // CTA-split path.  Launch order: split tiles, then the others.
+    std::vector<Item> launch_items;
+    int n_split = 0;
+    {
+        const int warps = engine_grid(ctx, engine_plain_variant()) * ENGINE_WARPS_PER_CTA;
+        std::vector<Item> keep;
+        if ((int64_t)items.size() < warps) {
+            for (const Item &t : items) {
+                const int M = t.src_end;
+                if (M < SPLIT_MIN_SOURCES * ENGINE_WARPS_PER_CTA) {
+                    keep.push_back(t);
+                    continue;
+                }
+                const int per = ((M + ENGINE_WARPS_PER_CTA - 1) / ENGINE_WARPS_PER_CTA +
+                                 SPLIT_MIN_SOURCES - 1) / SPLIT_MIN_SOURCES * SPLIT_MIN_SOURCES;
+                for (int w = 0; w < ENGINE_WARPS_PER_CTA; w++) {
+                    Item it = t;
+                    it.src_begin = std::min(M, w * per);
+                    it.src_end = std::min(M, (w + 1) * per);
+                    launch_items.push_back(it);
+                }
+                n_split++;
+            }
+        } else {
+            keep = items;
+        }
+        launch_items.insert(launch_items.end(), keep.begin(), keep.end());
+    }
+    nitems = launch_items.size();
     st = grow(ctx, b, (size_t)n_mini, (size_t)n_sinks, nitems, (size_t)ncell + 1);
     if (st != NF_OK) return st;
     // stage the source rows (each particle once) into pinned memory
@@ -367,7 +400,7 @@ static nf_status run_task(nf_ctx *ctx, SicBuffer &b, const SicTask &t) {
         }
     }
     memcpy(b.h_cs, cs.data(), cs.size() * sizeof(int64_t));
-    if (nitems) memcpy(b.h_items, items.data(), nitems * sizeof(Item));
+    if (nitems) memcpy(b.h_items, launch_items.data(), nitems * sizeof(Item));
     cudaStream_t sm = b.stream;
     size_t pb = (size_t)n_mini * sizeof(float);
     NF_CUDA(cudaMemcpyAsync(b.d_raw, hx, pb, cudaMemcpyHostToDevice, sm));
@@ -383,8 +416,10 @@ static nf_status run_task(nf_ctx *ctx, SicBuffer &b, const SicTask &t) {
     L.pos = b.d_pos;
     L.cs = b.d_cs;
     L.cpd = cpd;
-    L.light = b.d_items;
-    L.n_light = (int)nitems;
+    L.heavy = b.d_items;
+    L.n_heavy_groups = n_split;
+    L.light = b.d_items + (size_t)n_split * ENGINE_WARPS_PER_CTA;
+    L.n_light = (int)nitems - n_split * ENGINE_WARPS_PER_CTA;
     L.counters = b.d_counters;
     L.part = b.d_part;
     L.p0 = p0;
