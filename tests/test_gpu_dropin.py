@@ -161,3 +161,23 @@ def test_every_record_written(capi, synth, node):
         db.forces(0, box.cpd, out=out)
         db.close()
     assert np.all(np.isfinite(out))
+
+
+def test_sic_timing_counts_every_sic(capi, synth, oracle):
+    """nf_sic_timing: the summed pencil-kernel time of the SICs of a sweep,
+    their count and their unpadded pairs (the sweep's DirectTotal); a reset
+    zeroes the counters."""
+    box = synth.clustered_box(40000, 11, seed=44, n_clumps=20)
+    drv = capi.Driver(box, softening=1, softening_length=synth.plummer_eps(34), direct_bpd=2)
+    try:
+        drv.run_all()
+        ms, n, pairs = drv.sic_timing(reset=True)
+        st = drv.stats()
+        assert n >= box.cpd and ms > 0.0
+        assert pairs == st.direct_interactions == oracle.pair_count(box)
+        assert drv.sic_timing() == (0.0, 0, 0)
+        drv.run_all()
+        ms2, n2, pairs2 = drv.sic_timing()
+        assert n2 == n and pairs2 == pairs and ms2 > 0.0
+    finally:
+        drv.close()
