@@ -18,10 +18,10 @@
 // from float4 HBM records (register prefetch of the next chunk overlaps the
 // current chunk's math), each source read by every lane with broadcast
 // loads.  A lane evaluates its sinks two at a time with sm_100's paired FP32
-// instructions (f32x2).  Per 64-source chunk the FP32 partial is folded into
-// a TwoSum (hi, lo) pair.  A tile writes one double partial per sink and
+// instructions (f32x2).  Every 128 sources the FP32 partial is folded into
+// a compensated (hi, lo) pair.  A tile writes that pair per sink and
 // component into the sink's pencil slot; the co-add kernel sums the 2R+1
-// slots in a fixed order.
+// slots in a fixed order, in compensated FP32.
 //
 // Resident boxes are stored with the particles of each cell in Morton order
 // of their cell-relative position (the co-add writes results back in the
@@ -61,7 +61,7 @@ struct KParams {
     const Item *light;
     int n_light;
     int *counters;    // [0] heavy groups, [1] light items
-    double *part;     // [(2R+1) * nc][n_range]
+    Partial *part;    // [(2R+1) * nc][n_range] compensated (hi, lo) pairs
     int64_t p0, n_range;
     int nc;           // 3, or 4 with the density channel
     int plain;        // NF_ACC_PLAIN
@@ -228,10 +228,19 @@ __device__ __forceinline__ void chunk_paired(const float4 *bxy, const float2 *bz
     }
 }
 
-// Combine area for CTA-split tiles: [warp][component][sink] doubles.
+// Combine area for CTA-split tiles: [warp][component][sink] partials.
 struct CombSmem {
-    double v[WARPS_PER_CTA][4][TILE_MAX];
+    Partial v[WARPS_PER_CTA][4][TILE_MAX];
 };
+
+// (s, e) += the partial (hi, lo), compensated FP32: s the running sum, e
+// the running correction (the value is s + e).
+__device__ __forceinline__ void add_partial(float &s, float &e, Partial p) {
+    float t, err;
+    two_sum(s, p.x, t, err);
+    s = t;
+    e = e + (err + p.y);
+}
 
 // Particle index and pencil slot of sink i of the tile's pencil.
 __device__ __forceinline__ int64_t sink_particle(const WarpSmem &ws, int i, int &a) {
@@ -399,19 +408,20 @@ __device__ void run_tile(const KParams &kp, WarpSmem &ws, const Item &it, int la
     for (int s = 0; s < S; s++) {
         int j = s * 32 + lane;
         if (j >= it.nsink) continue;
-        double vx, vy, vz, vw = 0.0;
+        // the sink's running sums, kept as (hi, lo) pairs
+        Partial vx, vy, vz, vw = make_float2(0.f, 0.f);
         if constexpr (S == 1) {
-            vx = (double)hx1 + (double)lx1;
-            vy = (double)hy1 + (double)ly1;
-            vz = (double)hz1 + (double)lz1;
-            if (DENS) vw = (double)pw1;
+            vx = make_float2(hx1, lx1);
+            vy = make_float2(hy1, ly1);
+            vz = make_float2(hz1, lz1);
+            if (DENS) vw = make_float2(pw1, 0.f);
         } else {
             const int q = s >> 1;
             const bool odd = s & 1;
-            vx = (double)(odd ? hx[q].y : hx[q].x) + (double)(odd ? lx[q].y : lx[q].x);
-            vy = (double)(odd ? hy[q].y : hy[q].x) + (double)(odd ? ly[q].y : ly[q].x);
-            vz = (double)(odd ? hz[q].y : hz[q].x) + (double)(odd ? lz[q].y : lz[q].x);
-            if (DENS) vw = (double)(odd ? pw[q].y : pw[q].x);
+            vx = odd ? make_float2(hx[q].y, lx[q].y) : make_float2(hx[q].x, lx[q].x);
+            vy = odd ? make_float2(hy[q].y, ly[q].y) : make_float2(hy[q].x, ly[q].x);
+            vz = odd ? make_float2(hz[q].y, lz[q].y) : make_float2(hz[q].x, lz[q].x);
+            if (DENS) vw = make_float2(odd ? pw[q].y : pw[q].x, 0.f);
         }
         if (comb) {  // split tiles hold at most TILE_MAX sinks (host-built)
             if (j >= TILE_MAX) continue;
@@ -422,7 +432,7 @@ __device__ void run_tile(const KParams &kp, WarpSmem &ws, const Item &it, int la
         } else {
             int a;
             int64_t idx = sink_particle(ws, it.sink_begin + j, a) - kp.p0;
-            double *bp = kp.part + (int64_t)a * NC * kp.n_range + idx;
+            Partial *bp = kp.part + (int64_t)a * NC * kp.n_range + idx;
             bp[0] = vx;
             bp[kp.n_range] = vy;
             bp[2 * kp.n_range] = vz;
@@ -472,13 +482,13 @@ __global__ void __launch_bounds__(WARPS_PER_CTA * 32, MINB) pencil_kernel(KParam
         for (int j = threadIdx.x; j < it.nsink; j += blockDim.x) {
             int a;
             int64_t idx = sink_particle(w0, it.sink_begin + j, a) - kp.p0;
-            double *bp = kp.part + (int64_t)a * NC * kp.n_range + idx;
+            Partial *bp = kp.part + (int64_t)a * NC * kp.n_range + idx;
 #pragma unroll
             for (int c = 0; c < NC; c++) {
-                double v = 0.0;
+                float cs = 0.f, ce = 0.f;  // the warps' partials, summed in warp order
 #pragma unroll
-                for (int w = 0; w < WARPS_PER_CTA; w++) v += comb->v[w][c][j];
-                bp[(int64_t)c * kp.n_range] = v;
+                for (int w = 0; w < WARPS_PER_CTA; w++) add_partial(cs, ce, comb->v[w][c][j]);
+                bp[(int64_t)c * kp.n_range] = make_float2(cs, ce);
             }
         }
         __syncthreads();
@@ -499,20 +509,32 @@ __global__ void __launch_bounds__(WARPS_PER_CTA * 32, MINB) pencil_kernel(KParam
 // perm (optional): the caller's particle index of each packed slot; the
 // record of slot p0 + p goes to perm[p0 + p] - p0 (a permutation of the
 // range, since the in-cell ordering never moves a particle out of its cell).
-__global__ void coadd_kernel(const double *__restrict__ part, int64_t n, int W, int nc,
-                             double scale, int out_kind, void *out,
+// The 2R+1 partials of particle p of the range, summed in compensated FP32
+// in pencil-slot order; x, y, z times the output scale (one rounding: the
+// correction is scaled and added inside the FMA), w unscaled.
+__device__ __forceinline__ void coadd_sink(const Partial *__restrict__ part, int64_t n, int W,
+                                           int nc, int64_t p, float scale, float r[4]) {
+    float s[4] = {0.f, 0.f, 0.f, 0.f}, e[4] = {0.f, 0.f, 0.f, 0.f};
+    for (int a = 0; a < W; a++)
+#pragma unroll
+        for (int c = 0; c < 4; c++)
+            if (c < nc) add_partial(s[c], e[c], part[((int64_t)a * nc + c) * n + p]);
+#pragma unroll
+    for (int c = 0; c < 3; c++) r[c] = fmaf(s[c], scale, e[c] * scale);
+    r[3] = nc == 4 ? s[3] + e[3] : 0.f;
+}
+
+__global__ void coadd_kernel(const Partial *__restrict__ part, int64_t n, int W, int nc,
+                             float scale, int out_kind, void *out,
                              const uint32_t *__restrict__ perm, int64_t p0) {
     int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride) {
-        double v[4] = {0.0, 0.0, 0.0, 0.0};
-        for (int a = 0; a < W; a++)
-#pragma unroll
-            for (int c = 0; c < 4; c++)
-                if (c < nc) v[c] += part[((int64_t)a * nc + c) * n + p];
-        float x = (float)(v[0] * scale), y = (float)(v[1] * scale), z = (float)(v[2] * scale);
+        float r[4];
+        coadd_sink(part, n, W, nc, p, scale, r);
+        const float x = r[0], y = r[1], z = r[2];
         const int64_t o_i = perm ? (int64_t)perm[p0 + p] - p0 : p;
         if (out_kind == NF_OUT_FLOAT4) {
-            reinterpret_cast<float4 *>(out)[o_i] = make_float4(x, y, z, nc == 4 ? (float)v[3] : 0.f);
+            reinterpret_cast<float4 *>(out)[o_i] = make_float4(x, y, z, r[3]);
         } else {
             float *o = reinterpret_cast<float *>(out) + 3 * o_i;
             o[0] = x;
@@ -599,8 +621,8 @@ struct KickConst {
     float near_scale, rescale, kick1, kick2, b2;
 };
 
-__global__ void kick_kernel(const double *__restrict__ part, int64_t n, int W, int nc,
-                            double scale, const int64_t *__restrict__ cs, int64_t c0,
+__global__ void kick_kernel(const Partial *__restrict__ part, int64_t n, int W, int nc,
+                            float scale, const int64_t *__restrict__ cs, int64_t c0,
                             int64_t ncells, int64_t p0, const uint32_t *__restrict__ perm,
                             KickConst k, const float *__restrict__ far, float *vel, void *acc_out,
                             int out_kind, float *stats) {
@@ -612,13 +634,9 @@ __global__ void kick_kernel(const double *__restrict__ part, int64_t n, int W, i
         float sv2 = 0.f, mv = 0.f, ma = 0.f;
         for (int64_t slot = s0 + lane; slot < s1; slot += 32) {
             const int64_t i = slot - p0;
-            double v[4] = {0.0, 0.0, 0.0, 0.0};
-            for (int a = 0; a < W; a++)
-#pragma unroll
-                for (int q = 0; q < 4; q++)
-                    if (q < nc) v[q] += part[((int64_t)a * nc + q) * n + i];
-            const float nx = (float)(v[0] * scale), ny = (float)(v[1] * scale),
-                        nz = (float)(v[2] * scale), nw = nc == 4 ? (float)v[3] : 0.f;
+            float r[4];
+            coadd_sink(part, n, W, nc, i, scale, r);
+            const float nx = r[0], ny = r[1], nz = r[2], nw = r[3];
             const int64_t o = perm ? (int64_t)perm[slot] - p0 : i;
             const float fx = far ? far[3 * o] : 0.f, fy = far ? far[3 * o + 1] : 0.f,
                         fz = far ? far[3 * o + 2] : 0.f;
@@ -955,11 +973,13 @@ static KParams make_params(nf_ctx *ctx, nf_box *box, const Plan &pl) {
     return params_from(ctx, L);
 }
 
-// eps: the softening parameter in use (0: the context's)
-static double output_scale(const nf_config &cfg, float eps = 0.f) {
+// Output scale of the co-add, formed in double on the host and rounded once
+// to float (single spline: eps_int^3, the raw kernel's units; otherwise 1).
+// eps: the softening parameter in use (0: the context's).
+static float output_scale(const nf_config &cfg, float eps = 0.f) {
     if (eps <= 0.f) eps = cfg.eps;
-    if (cfg.softening == SOFT_SINGLE_SPLINE) return pow((double)eps, -1.5);  // eps_int^3
-    return 1.0;
+    if (cfg.softening == SOFT_SINGLE_SPLINE) return (float)pow((double)eps, -1.5);  // eps_int^3
+    return 1.0f;
 }
 
 int engine_variant_smax(int variant) { return VARIANTS[variant].smax; }
@@ -992,7 +1012,7 @@ nf_status engine_launch(nf_ctx *ctx, const EngineLaunch &L, double, cudaStream_t
     return NF_OK;
 }
 
-nf_status engine_coadd(nf_ctx *ctx, const double *part, int64_t n, void *out, cudaStream_t st,
+nf_status engine_coadd(nf_ctx *ctx, const Partial *part, int64_t n, void *out, cudaStream_t st,
                        float eps, const uint32_t *perm, int64_t p0) {
     if (n <= 0) return NF_OK;
     const nf_config &cfg = ctx->cfg;
@@ -1327,12 +1347,12 @@ extern "C" nf_status nf_box_pair_count(nf_ctx *ctx, const nf_box *box, int lo, i
     return NF_OK;
 }
 
-// Partial scratch: (2R+1) slots x nc components x n_range doubles, shared by
+// Partial scratch: (2R+1) slots x nc components x n_range (hi, lo) pairs, shared by
 // the box's plans (grown on demand; cached graphs that refer to the old
 // buffer are dropped).
 static nf_status ensure_scratch(nf_ctx *ctx, nf_box *box, int64_t n_range) {
     int nc = ctx->cfg.b2 > 0.f ? 4 : 3;
-    size_t need = (size_t)(2 * ctx->cfg.near_field_radius + 1) * nc * (size_t)n_range * sizeof(double);
+    size_t need = (size_t)(2 * ctx->cfg.near_field_radius + 1) * nc * (size_t)n_range * sizeof(Partial);
     if (need <= box->part_bytes) return NF_OK;
     cudaFree(box->d_part);
     box->d_part = nullptr;
@@ -1652,9 +1672,10 @@ namespace nf {
 constexpr int64_t NOALLOC_MAX_SINKS = 196608;             // particles per call
 constexpr size_t NOALLOC_SCRATCH_BYTES = (size_t)32 << 20;  // 32 MiB
 constexpr size_t NOALLOC_COUNTER_BYTES = 256;
-static_assert(NOALLOC_COUNTER_BYTES + (size_t)MAXW * 4 * 8 * NOALLOC_MAX_SINKS <= NOALLOC_SCRATCH_BYTES,
-              "scratch holds (2R+1) x 4 double partials per sink");
-// [0, 256): work counters; then (2R+1) x nc x n doubles of pencil partials.
+static_assert(NOALLOC_COUNTER_BYTES + (size_t)MAXW * 4 * sizeof(Partial) * NOALLOC_MAX_SINKS <=
+                  NOALLOC_SCRATCH_BYTES,
+              "scratch holds (2R+1) x 4 pencil partials per sink");
+// [0, 256): work counters; then (2R+1) x nc x n pencil partials.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
 
 // Warps take whole pencils from a counter and run their tiles in order.
@@ -1770,7 +1791,7 @@ extern "C" nf_status nf_forces_noalloc(const nf_config *cfg, int cpd, const void
     L.cs = cell_start;
     L.cpd = cpd;
     L.counters = (int *)base;
-    L.part = (double *)((char *)base + NOALLOC_COUNTER_BYTES);
+    L.part = (Partial *)((char *)base + NOALLOC_COUNTER_BYTES);
     L.p0 = bounds[0];
     L.n_range = n;
     KParams kp = params_from(&tmp, L);

@@ -27,6 +27,11 @@ nf_status cuda_fail(cudaError_t e, const char *what);
         if (_e != cudaSuccess) return nf::cuda_fail(_e, #call); \
     } while (0)
 
+// A pencil partial of one sink and component: a compensated FP32 sum kept as
+// (hi, lo), value hi + lo.  The co-add sums the 2R+1 partials of a sink with
+// compensated FP32 arithmetic too, so no FP64 enters the accumulation.
+typedef float2 Partial;
+
 // One warp work item of the pencil kernel (32 bytes).
 struct Item {
     int32_t pencil;      // linear id of the pencil's centre cell (x, y, zc)
@@ -67,7 +72,7 @@ struct EngineLaunch {
     const Item *light = nullptr;
     int n_light = 0;
     int *counters = nullptr;      // 2 ints, zeroed by engine_launch
-    double *part = nullptr;       // (2R+1) * nc * n_range doubles
+    Partial *part = nullptr;      // (2R+1) * nc * n_range partials
     int64_t p0 = 0, n_range = 0;  // the sinks' particle range
     int variant = 0;
     int grid = 0;                 // CTAs (0: one full wave)
@@ -76,7 +81,7 @@ struct EngineLaunch {
 nf_status engine_launch(nf_ctx *ctx, const EngineLaunch &L, double box_h, cudaStream_t st);
 // perm (optional): the caller's index of each packed slot; record p of the
 // range [p0, p0 + n) is written at perm[p0 + p] - p0.
-nf_status engine_coadd(nf_ctx *ctx, const double *part, int64_t n, void *out, cudaStream_t st,
+nf_status engine_coadd(nf_ctx *ctx, const Partial *part, int64_t n, void *out, cudaStream_t st,
                        float eps = 0.f, const uint32_t *perm = nullptr, int64_t p0 = 0);
 nf_status engine_pack(nf_ctx *ctx, const float *x, const float *y, const float *z, int64_t n,
                       float4 *out, cudaStream_t st);
@@ -101,7 +106,7 @@ struct nf_box {
     std::vector<int64_t> cell_start;  // host copy, cpd^3 + 1
     float4 *d_pos = nullptr;          // np records (x, y, z, 0), cell order
     int64_t *d_cs = nullptr;          // cell_start on the device
-    double *d_part = nullptr;         // pencil partials scratch
+    nf::Partial *d_part = nullptr;    // pencil partials scratch
     float *d_stage = nullptr;         // position upload staging, 3 * np floats
     uint32_t *d_perm = nullptr;       // caller's index of the particle in each packed slot
     void *d_sort = nullptr;           // in-cell ordering scratch (keys, values, sort temp)

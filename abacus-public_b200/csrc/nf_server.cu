@@ -33,7 +33,7 @@ struct Req;
 struct Slot {
     int index = 0;
     cudaStream_t stream = nullptr;
-    double *part = nullptr;
+    Partial *part = nullptr;
     void *out = nullptr;
     int *counters = nullptr;
     size_t part_cap = 0, out_cap = 0;  // bytes
@@ -137,12 +137,12 @@ struct Booking {
     std::vector<void *> release_ptrs;  // their buffers, taken at booking time
 };
 
-// Device bytes of a slab request: partials (one record of nc doubles per
+// Device bytes of a slab request: partials (one record of nc (hi, lo) pairs per
 // sink and pencil slot) and the output records.
 static void request_bytes(const nf_server *s, int64_t nsink, size_t *part, size_t *out) {
     const int W = 2 * s->ctx->cfg.near_field_radius + 1;
     const int nc = s->ctx->cfg.b2 > 0.f ? 4 : 3;
-    *part = (size_t)W * nc * (size_t)nsink * sizeof(double) + 16;
+    *part = (size_t)W * nc * (size_t)nsink * sizeof(Partial) + 16;
     *out = (size_t)nsink * rec_bytes(s->ctx) + 16;
 }
 
@@ -224,7 +224,7 @@ static nf_status apply_booking(nf_server *s, Booking &bk) {
         set_error("nf_server: device allocation failed within the HBM budget");
         return NF_ENOMEM;
     }
-    sl.part = (double *)p;
+    sl.part = (Partial *)p;
     sl.out = o;
     sl.counters = (int *)c;
     return NF_OK;

@@ -16,7 +16,7 @@
 //      slabs with the SIC's cell offsets;
 //   3. one launch of the pencil engine (the reference's block shape: tiles of
 //      64 sinks, in SIC order, no splitting, no graph) writes per-pencil
-//      double partials, and the co-add kernel sums the 2R+1 pencils of each
+//      compensated FP32 partials, and the co-add kernel sums the 2R+1 pencils of each
 //      sink on the device (PencilPlan.cc:140-207 co-adds on the host);
 //   4. the rows' accelerations are copied back and stored into AccSlab.
 #include <algorithm>
@@ -50,7 +50,7 @@ struct SicBuffer {
     float4 *d_pos = nullptr;
     int64_t *d_cs = nullptr;
     Item *d_items = nullptr;
-    double *d_part = nullptr;
+    Partial *d_part = nullptr;
     void *d_out = nullptr;
     int *d_counters = nullptr;
     float *h_raw = nullptr;
@@ -136,7 +136,7 @@ static nf_status grow(nf_ctx *ctx, SicBuffer &b, size_t particles, size_t sinks,
         b.d_out = nullptr;
         b.h_out = nullptr;
         b.cap_sinks = 0;
-        NF_CUDA(cudaMalloc(&b.d_part, (size_t)W * nc * c * sizeof(double)));
+        NF_CUDA(cudaMalloc(&b.d_part, (size_t)W * nc * c * sizeof(Partial)));
         NF_CUDA(cudaMalloc(&b.d_out, c * rec));
         NF_CUDA(host_alloc(&b.h_out, c * rec, b.pinned, false));
         b.cap_sinks = c;
