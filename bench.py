@@ -777,6 +777,8 @@ def our_arm(args, w):
         "slab_latency_ms": None if lvl1 is None else {
             "p50": lvl1["p50_ms"], "p99": lvl1["p99_ms"], "n": lvl1["requests"],
             "queue_p99": lvl1["queue_p99_ms"], "run_p99": lvl1["run_p99_ms"],
+            "solo_p50": serving["solo_service_ms"]["p50"],
+            "solo_p99": serving["solo_service_ms"]["p99"],
             "what": "serving at 0.5x measured capacity: Poisson slab requests over the "
                     "resident boxes, submit to result in the caller's device buffer"},
         "serving": serving,
