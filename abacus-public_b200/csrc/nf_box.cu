@@ -1394,8 +1394,9 @@ static nf_status time_pencil(nf_ctx *ctx, nf_box *box, Plan &pl, float *ms) {
 }
 
 // The autotuner: run every candidate kernel shape on the requested slab
-// range (one warm-up launch, one timed launch each) and keep the fastest
-// for the box.
+// range and keep the fastest for the box.  A candidate whose first launch
+// is short (< 50 ms, where loading the kernel and a cold L2 weigh) is timed
+// again and the second launch counts; a long first launch counts as it is.
 static nf_status autotune(nf_ctx *ctx, nf_box *box, int lo, int hi) {
     const bool tun = tunable(ctx->cfg.softening, ctx->cfg.b2 > 0.f);
     const int nv = tun ? NVARIANTS : 1;
@@ -1407,7 +1408,7 @@ static nf_status autotune(nf_ctx *ctx, nf_box *box, int lo, int hi) {
         if (st != NF_OK) return st;
         float ms = 0;
         st = time_pencil(ctx, box, *pl, &ms);
-        if (st == NF_OK) st = time_pencil(ctx, box, *pl, &ms);
+        if (st == NF_OK && ms < 50.f) st = time_pencil(ctx, box, *pl, &ms);
         free_plan(*pl);
         if (st != NF_OK) return st;
         box->tune_ms[v] = ms;
