@@ -56,3 +56,28 @@ def test_parity_vs_reference_bound(synth):
     got[4, 1] = ref[4, 1]
     got[5, 1] += 1.0  # an unsampled sink does not count
     assert bench.parity_vs_reference(got, ref, sinks)["pass"]
+
+
+def test_both_arms_report_one_workload_config(synth):
+    """The reference arm and this arm describe the same workload with the
+    same config dict (the driver compares them); the L2 note follows the
+    box size."""
+    import argparse
+    bench = _bench()
+    args = argparse.Namespace(workload="clustered512")
+    box = synth.clustered_box(40000, 11, seed=3, n_clumps=20)
+    pairs = int(bench.cell_pairs(box).sum())
+    a = bench.workload_config(args, bench.WORKLOADS["clustered512"], box, pairs)
+    b = bench.workload_config(args, bench.WORKLOADS["clustered512"], box, pairs, 1)
+    assert a == b and a["pairs_per_step_per_gpu"] == pairs and a["particles_per_gpu"] == box.n
+    assert "fit in L2" in a["l2"]  # 40,000 particles: 5.4 MB of inputs
+
+
+def test_roofline_peak_is_the_larger_of_probe_and_clock():
+    bench = _bench()
+    peak, derived = bench.peak_from(72.0, {"sm_mhz": 1965.0}, 148)
+    assert abs(derived - 148 * 128 * 2 * 1965e6 / 1e12) < 1e-9 and peak == derived
+    peak, _ = bench.peak_from(80.0, {"sm_mhz": 1965.0}, 148)
+    assert peak == 80.0
+    peak, derived = bench.peak_from(72.0, {"sm_mhz": None}, 148)
+    assert peak == 72.0
