@@ -360,13 +360,15 @@ def percentile(xs, q):
     return float(np.percentile(np.asarray(xs), q)) if xs else None
 
 
-def plain_dropin(capi, box, w, device, a_batched=None, steps=2):
+def plain_dropin(capi, box, w, device, a_batched=None, steps=2, fp64=None):
     """The plain drop-in: the NearFieldDriver mirror (SIC planning, y-splits,
     one launch per SIC, host slabs staged per SIC, AccSlab written back) over
     every slab of the box.  Wall clock per full sweep with DirectBPD 3, then
     one sweep with DirectBPD 1 (SICs one after another) for the summed
     pencil-kernel time of its SICs.  a_batched: the batched sweep's result, to
-    compare the drop-in's output with."""
+    compare the drop-in's output with (over every sink; the sink where they
+    differ most is checked against the FP64 oracle too).  fp64 = (sinks,
+    FP64 accelerations): the drop-in's own error on those sinks."""
     from abacus_public_b200 import synth
     length = synth.plummer_eps(w["n_side"])
     drv = capi.Driver(box, softening=w["softening"], softening_length=length, device=device,
@@ -385,11 +387,24 @@ def plain_dropin(capi, box, w, device, a_batched=None, steps=2):
                "splits_per_slab": st.mean_splits_per_slab, "buffers": st.nbuffers,
                "gb_to_device_per_step": st.total_gb_to / (steps + 1),
                "what": "host slabs -> NearFieldDriver -> SIC -> AccSlab, wall clock"}
+        sys.path.insert(0, str(ROOT / "oracle"))
+        import oracle
         if a_batched is not None:
             ref = np.asarray(a_batched[:, :3], np.float64)
             norm = np.maximum(np.linalg.norm(ref, axis=1), 1e-300)
-            res["max_comp_rel_vs_batched"] = float(
-                (np.abs(acc[:, :3] - ref).max(axis=1) / norm).max())
+            rel = np.abs(acc[:, :3] - ref).max(axis=1) / norm
+            k = int(np.argmax(rel))
+            res["max_comp_rel_vs_batched"] = float(rel[k])
+            a64 = oracle.fp64_sinks(box, w["softening"], kernel_eps(w), np.array([k]))
+            m64 = float(np.linalg.norm(a64))
+            med = float(np.median(norm[::max(1, box.n // 100000)]))
+            res["worst_sink"] = {
+                "sink": k, "abs_a_over_median": m64 / med,
+                "plain_frac_err_vs_fp64": float(np.linalg.norm(acc[k, :3] - a64[0]) / m64),
+                "batched_frac_err_vs_fp64": float(np.linalg.norm(ref[k] - a64[0]) / m64)}
+        if fp64 is not None:
+            rms, mx, _ = oracle.frac_errors(acc[fp64[0], :3], fp64[1])
+            res["vs_fp64"] = {"rms_frac": rms, "max_frac": mx, "sinks": int(fp64[0].size)}
         del acc
     finally:
         drv.close()
@@ -740,7 +755,8 @@ def our_arm(args, w):
         precision, fp64 = ph.run("precision_study", precision_study, capi, box, w, local,
                                  stream, args.precision_steps, oa, tv)
     if rank == 0 and not args.no_plain:
-        plain = ph.run("plain_dropin", plain_dropin, capi, box, w, local, a_batched=oa)
+        plain = ph.run("plain_dropin", plain_dropin, capi, box, w, local, a_batched=oa,
+                       fp64=fp64)
         plain["batched_over_plain"] = e2e_value / plain["value"]
         plain["batched_over_plain_what"] = "e2e (nf_box_step from pinned host buffers) over " \
                                            "the drop-in's wall clock, same box"
