@@ -273,6 +273,25 @@ def cpu_sample(box, target_pairs, seed=CPU_SAMPLE_SEED):
     return cells, sinks, pairs, desc
 
 
+def host_cpu():
+    """The host CPU the baseline ran on: model name, logical CPUs of the host
+    and the ones this process may use (the threads the baseline takes)."""
+    model = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    try:
+        usable = len(os.sched_getaffinity(0))
+    except AttributeError:  # pragma: no cover
+        usable = os.cpu_count()
+    return {"model": model, "host_logical_cpus": os.cpu_count(), "usable_cpus": usable}
+
+
 def cpu_reference_run(box, w, cells, threads):
     """The reference CPU direct on the sample's cells: (float32[N, 3] with the
     sample's rows written, seconds, kind)."""
@@ -348,7 +367,7 @@ def reference_arm(args, w):
         "step": "the reference CPU direct on a fixed seeded sample of sink cells of the box "
                 "(a whole sweep takes hours on the host)",
         "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": threads, "kind": kind,
-                         "sample": desc},
+                         "sample": desc, "cpu": host_cpu()},
         "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -827,7 +846,8 @@ def our_arm(args, w):
         cells, sinks, spairs, desc = cpu_sample(box, args.cpu_pairs)
         a_ref, dt, kind = ph.run("cpu_baseline", cpu_reference_run, box, w, cells, threads)
         result["cpu_baseline"] = {"value": spairs / dt, "unit": "pairs/s", "cores": threads,
-                                  "kind": kind, "sample": f"{desc}, {dt:.1f} s"}
+                                  "kind": kind, "sample": f"{desc}, {dt:.1f} s",
+                                  "cpu": host_cpu()}
         result["parity_vs_reference"] = dict(
             parity_vs_reference(oa, a_ref, sinks),
             reference="the reference CPU direct (Direct::Execute, -Ofast build) on the "

@@ -81,3 +81,10 @@ def test_roofline_peak_is_the_larger_of_probe_and_clock():
     assert peak == 80.0
     peak, derived = bench.peak_from(72.0, {"sm_mhz": None}, 148)
     assert peak == 72.0
+
+
+def test_cpu_baseline_names_the_host_cpu():
+    bench = _bench()
+    cpu = bench.host_cpu()
+    assert set(cpu) == {"model", "host_logical_cpus", "usable_cpus"}
+    assert 1 <= cpu["usable_cpus"] <= cpu["host_logical_cpus"]
