@@ -1,4 +1,4 @@
-"""Known answers on the GPU path (the survey's pair-kernel checks):
+"""Known answers on the GPU path (pair-kernel checks at the softening edges):
 two bodies at r = 0, r < eps (the single spline's near branch), r = eps,
 r > eps and one cell apart, against the softening formulas evaluated in
 double; and the cubic lattice, whose symmetric 5x5x5 neighbourhoods cancel
