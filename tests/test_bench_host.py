@@ -60,8 +60,8 @@ def test_parity_vs_reference_bound(synth):
 
 def test_both_arms_report_one_workload_config(synth):
     """The reference arm and this arm describe the same workload with the
-    same config dict (the driver compares them); the L2 note follows the
-    box size."""
+    same config dict (a ratio of the two lines needs one workload); the L2
+    note follows the box size."""
     import argparse
     bench = _bench()
     args = argparse.Namespace(workload="clustered512")
