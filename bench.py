@@ -28,6 +28,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import pathlib
 import statistics
@@ -371,8 +372,22 @@ def reference_arm(args, w):
         "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
-    print(json.dumps(line), flush=True)
+    print(json_line(line), flush=True)
     return 0
+
+
+def json_line(obj):
+    """One strict-JSON line: NaN and infinities (a ratio with an empty
+    denominator, say) become null."""
+    def clean(v):
+        if isinstance(v, float) and not math.isfinite(v):
+            return None
+        if isinstance(v, dict):
+            return {k: clean(x) for k, x in v.items()}
+        if isinstance(v, (list, tuple)):
+            return [clean(x) for x in v]
+        return v
+    return json.dumps(clean(obj), allow_nan=False)
 
 
 def percentile(xs, q):
@@ -657,9 +672,11 @@ class Phases:
 
 
 def peak_from(sust, clocks, sms):
-    """max(probe, clock-derived) for an already measured probe value."""
+    """max(probe, clock-derived) for an already measured probe value; the
+    clock-derived peak is None when no clock sample fell in the timed region
+    (a timed region shorter than the sampling period)."""
     mhz = clocks.get("sm_mhz") if isinstance(clocks, dict) else None
-    derived = sms * 128 * 2 * mhz * 1e6 / 1e12 if mhz else float("nan")
+    derived = sms * 128 * 2 * mhz * 1e6 / 1e12 if mhz else None
     return (max(sust, derived) if mhz else sust), derived
 
 
@@ -669,7 +686,7 @@ def fp32_peaks(ctx, clocks, sms):
     in the timed region; the larger of the two is used."""
     burst, sust = ctx.fp32_peak(1.0)
     mhz = clocks.get("sm_mhz") if isinstance(clocks, dict) else None
-    derived = sms * 128 * 2 * mhz * 1e6 / 1e12 if mhz else float("nan")
+    derived = sms * 128 * 2 * mhz * 1e6 / 1e12 if mhz else None
     peak = max(sust, derived) if mhz else sust
     src = ("clock-derived: %d SMs x 128 FP32 lanes x 2 flops x %.0f MHz (median SM clock "
            "sampled in the timed region)" % (sms, mhz)) if mhz and derived >= sust else \
@@ -856,7 +873,7 @@ def our_arm(args, w):
     result["phase_s"] = ph.t
     ctx.close()
     if rank == 0:
-        print(json.dumps(result), flush=True)
+        print(json_line(result), flush=True)
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
@@ -941,7 +958,7 @@ def big_arm(args, w):
     }
     db.close()
     ctx.close()
-    print(json.dumps(result), flush=True)
+    print(json_line(result), flush=True)
     return 0
 
 
@@ -1012,7 +1029,7 @@ def big_full_sweep(args, w, capi, ctx, db, hbox, eps, peak_s, stream):
         "accuracy_vs_fp64": {"rms_frac": c["rms_frac"], "max_frac": c["max_frac"], "sinks": 2000},
         "gpu_launches": 2 * len(ranges) * 2,
     }
-    print(json.dumps(result), flush=True)
+    print(json_line(result), flush=True)
     return 0
 
 
@@ -1116,7 +1133,7 @@ def shard_arm(args, w):
     db.close()
     ctx.close()
     if rank == 0:
-        print(json.dumps(result), flush=True)
+        print(json_line(result), flush=True)
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()

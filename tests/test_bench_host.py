@@ -80,7 +80,7 @@ def test_roofline_peak_is_the_larger_of_probe_and_clock():
     peak, _ = bench.peak_from(80.0, {"sm_mhz": 1965.0}, 148)
     assert peak == 80.0
     peak, derived = bench.peak_from(72.0, {"sm_mhz": None}, 148)
-    assert peak == 72.0
+    assert peak == 72.0 and derived is None  # JSON null, never NaN
 
 
 def test_cpu_baseline_names_the_host_cpu():
