@@ -88,3 +88,10 @@ def test_cpu_baseline_names_the_host_cpu():
     cpu = bench.host_cpu()
     assert set(cpu) == {"model", "host_logical_cpus", "usable_cpus"}
     assert 1 <= cpu["usable_cpus"] <= cpu["host_logical_cpus"]
+
+
+def test_bench_lines_are_strict_json():
+    import json
+    bench = _bench()
+    line = bench.json_line({"a": float("nan"), "b": [1.0, float("inf")], "c": {"d": -float("inf")}})
+    assert json.loads(line) == {"a": None, "b": [1.0, None], "c": {"d": None}}
